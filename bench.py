@@ -1,0 +1,306 @@
+"""Benchmark of the effective-Hamiltonian matvec (Heff TFLOP/s).
+
+One step = one matvec Psi' = Heff Psi over one optimisation step of the
+synthetic 24-orbital quantum-chemistry Hamiltonian at D=512 (U1 x SU2,
+SITE_SIZE 2; step files captured from the reference sweep, operator values
+and schedule exactly as the reference builds them).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+The engine arm times K matvecs with CUDA events on the launching stream
+(inputs resident in HBM; L2 flushed between iterations by writing a 256 MiB
+buffer), then the same through the host-buffer C-ABI call (`e2e`: pinned
+host x -> device -> matvec -> host y).  The reference arm times the
+reference's own matvecT3NS (exec_secondrun, OpenMP + OpenBLAS) on the host
+cores for the same step.  Multi-GPU runs are independent replicas (the
+matvec of one step is not sharded), value = total FLOPs / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Heff TFLOP/s"
+UNIT = "TFLOP/s"
+DEFAULT_WORKLOAD_DIR = os.path.join(ROOT, "oracle", "_ref", "captures", "qc24_D512")
+
+
+def pick_workload(path: str | None) -> str:
+    if path:
+        return path
+    cands = sorted(glob.glob(os.path.join(DEFAULT_WORKLOAD_DIR, "*.t3c")),
+                   key=os.path.getsize)
+    if not cands:
+        raise SystemExit(f"no step files under {DEFAULT_WORKLOAD_DIR}; run "
+                         "python -m oracle.captures in the build container")
+    return cands[-1]
+
+
+def step_stats(s):
+    bb = s["beginblock"]
+    sizes = np.diff(bb)
+    return {"blocks": int(s["nrblocks"][0]), "psi_elems": int(bb[-1]),
+            "block_median": float(np.median(sizes)), "block_max": int(sizes.max()),
+            "merge_instr": int(s["iset.nr_instr"][0])}
+
+
+class Clocks:
+    """nvidia-smi sampler during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return None
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measure_fp64_peak(torch):
+    """cuBLAS DGEMM 8192^3 through torch (best of 5): the FP64 roofline."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_engine(args, rank, world):
+    import torch
+
+    from t3ns_b200.native import HeffPlan, StepDesc
+    from t3ns_b200.stepfile import read_step
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    path = pick_workload(args.workload)
+    s = read_step(path)
+    desc = StepDesc(s)
+    plan = HeffPlan(desc)
+    st = plan.stats
+    n = plan.size
+    g = torch.Generator(device="cpu").manual_seed(1234 + rank)
+    x = torch.randn(n, generator=g, dtype=torch.float64)
+    x /= x.norm()
+    x = x.cuda()
+    y = torch.empty_like(x)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    peak = measure_fp64_peak(torch) if rank == 0 else None
+
+    for _ in range(args.warmup):
+        plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+    times = []
+    with Clocks(dev) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+    t_steps = [a.elapsed_time(b) * 1e-3 for a, b in times]
+    t_total = float(sum(t_steps))
+    launches = plan.last_launches() * args.steps
+
+    # e2e: host buffers (pinned) through the C-ABI host entry point
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    import ctypes as C
+    lib = plan.lib
+    f64p = C.POINTER(C.c_double)
+    for _ in range(max(1, args.warmup // 2)):
+        lib.t3ns_heff_matvec_host(plan.h, C.cast(xh.data_ptr(), f64p), C.cast(yh.data_ptr(), f64p))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rc = lib.t3ns_heff_matvec_host(plan.h, C.cast(xh.data_ptr(), f64p),
+                                       C.cast(yh.data_ptr(), f64p))
+        if rc < 0:
+            raise RuntimeError(lib.t3ns_last_error())
+    t_e2e = time.perf_counter() - t0
+    err = float((yh.cuda() - y).norm() / y.norm())
+    assert err < 1e-12, err
+
+    if world > 1:
+        tt = torch.tensor([t_total, t_e2e], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_total, t_e2e = float(tt[0]), float(tt[1])
+    if rank != 0:
+        return None
+    flops = st["flops_ref"]
+    value = flops * args.steps * world / t_total / 1e12
+    achieved = flops / (t_total / args.steps) / 1e12
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "synthetic QC 24 orbitals, 24 e-, U1xSU2, D=512, SITE_SIZE 2: "
+                               "one step's Heff matvec (" + os.path.basename(path) + ")",
+                   **step_stats(s), "flops_per_matvec": flops,
+                   "parallelism": f"replicas{world}", "l2": "flushed between iterations",
+                   "precision": "fp64"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "peak_source": "measured this run: cuBLAS DGEMM 8192^3 via torch (FP64 "
+                                    "peak; MEASURED_PEAKS.json has no FP64 figure)"},
+        "e2e": {"value": flops * args.steps * world / t_e2e / 1e12, "unit": UNIT,
+                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    return out
+
+
+def cpu_baseline(path, samples=1):
+    """The reference's own matvecT3NS (exec_secondrun) on the host cores."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_matvec_bench")
+    if not os.path.exists(exe):
+        return None
+    ncores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(ncores), OPENBLAS_NUM_THREADS="1")
+    r = subprocess.run([exe, path, str(samples)], capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        return None
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    res["cores"] = ncores
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        path = pick_workload(args.workload)
+        from t3ns_b200.stepfile import read_step
+        s = read_step(path)
+        flops = None
+        res = cpu_baseline(path, samples=max(1, args.steps))
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build "
+                              "(oracle/_ref/ref_matvec_bench) missing"}))
+            return
+        flops = res["flops"]
+        v = flops / res["seconds_per_matvec"] / 1e12
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * res["seconds_per_matvec"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": os.path.basename(path), **step_stats(s)},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["cores"], "kind": "reference",
+                             "sample": f"{res['calls']} calls of the reference matvecT3NS "
+                                       "(exec_secondrun) on this step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    out = run_engine(args, rank, world)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(pick_workload(args.workload), samples=1)
+            if cb:
+                v = cb["flops"] / cb["seconds_per_matvec"] / 1e12
+                out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb["cores"],
+                                       "kind": "reference",
+                                       "sample": "1 call of the reference matvecT3NS "
+                                                 "(exec_secondrun) on the same step"}
+            else:
+                out["cpu_baseline"] = None
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

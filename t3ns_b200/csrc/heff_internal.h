@@ -1,0 +1,72 @@
+// Internal data structures of the matvec engine (host plan, device plan).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "t3ns_b200.h"
+
+namespace t3ns {
+
+// One (new block, old block, instruction) term: op_off[j] is the element
+// offset, in the device operator buffer, of the operator block acting on
+// memory axis j; `axes` packs the contraction sequence (2 bits per stage,
+// stage count in bits 6-7); pref = instruction prefactor * symmetry prefactor.
+struct __align__(16) HeffTask {
+        int64_t op_off[3];
+        double pref;
+        int old;
+        int axes;
+};
+
+struct HostPlan {
+        int isdmrg = 0;
+        int map[3] = {0, 1, 2};
+        int nblocks = 0;
+        int64_t size = 0;
+        std::vector<int64_t> block_off;
+        std::vector<int4> edims;                  // memory-axis dims per block
+        std::vector<std::vector<int64_t>> op_base;  // [set][op] element base
+        int64_t op_elems = 0;
+        std::vector<int> task_ptr;
+        std::vector<HeffTask> tasks;
+        std::vector<int> work_order;
+        int64_t npairs = 0;
+        int64_t max_w1 = 0, max_w2 = 0;
+        double flops_ref = 0, flops_exec = 0, bytes_alg = 0;
+};
+
+struct DevicePlan {
+        int nblocks = 0;
+        int64_t size = 0;
+        double *ops = nullptr;
+        int64_t *blk_off = nullptr;
+        int4 *edims = nullptr;
+        int *work_order = nullptr;
+        int n_active = 0;
+        int *task_ptr = nullptr;
+        HeffTask *tasks = nullptr;
+        double *scratch = nullptr;
+        int64_t scratch_w1 = 0, scratch_w2 = 0;
+        int grid = 0;
+        int *err = nullptr;
+};
+
+int build_plan(const t3ns_heff_desc *d, HostPlan &hp);
+int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStream_t s,
+                     int *launches);
+int launch_heff_diag(const DevicePlan &dp, double *diag, cudaStream_t s);
+
+}  // namespace t3ns
+
+struct t3ns_heff {
+        t3ns::HostPlan hp;
+        t3ns::DevicePlan dp;
+        int precision = T3NS_PREC_FP64;
+        int device = 0;
+        int last_launches = 0;
+        double *stage_x = nullptr;   // device staging for host-buffer calls
+        double *stage_y = nullptr;
+        cudaStream_t stream = nullptr;
+        std::vector<void *> allocs;
+};

@@ -1,0 +1,55 @@
+"""Reader for step-description files (``*.t3c``).
+
+A step file holds everything the effective-Hamiltonian matvec of one
+optimisation step needs, exactly as the reference sweep driver hands it to
+``init_Heffdata`` (reference ``include/Heff.h:54-155``): the multi-site tensor
+structure, the symsecs of every bond, the two or three renormalised operator
+sets with their block tables and elements, the merge instruction set
+(``include/instructions.h:39-66``), plus the replay schedule the reference built
+for that step (``struct secondrun``, ``include/Heff.h:36-51``) and reference
+matvec / diagonal / Davidson outputs.
+
+Layout: the 8-byte magic ``T3NSCAP1`` followed by records
+``{char name[48]; int32 dtype; int32 pad; int64 count; payload}`` with dtype
+1 = int32, 2 = int64, 3 = float64, little endian.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+_DTYPES = {1: np.int32, 2: np.int64, 3: np.float64}
+_HDR = np.dtype([("name", "S48"), ("dtype", "<i4"), ("pad", "<i4"), ("count", "<i8")])
+
+
+def read_step(path) -> dict:
+    """Return ``{name: ndarray}`` for every record of a step file."""
+    with open(path, "rb") as f:
+        buf = f.read()
+    if buf[:8] != b"T3NSCAP1":
+        raise ValueError(f"{path}: not a step file")
+    out = {}
+    pos = 8
+    while pos < len(buf):
+        hdr = np.frombuffer(buf, _HDR, 1, pos)[0]
+        pos += _HDR.itemsize
+        dt = np.dtype(_DTYPES[int(hdr["dtype"])])
+        n = int(hdr["count"])
+        arr = np.frombuffer(buf, dt, n, pos).copy()
+        pos += n * dt.itemsize
+        out[hdr["name"].decode()] = arr
+    return out
+
+
+def write_step(path, rec: dict) -> None:
+    """Write ``{name: ndarray}`` in the step-file layout (int32/int64/float64)."""
+    codes = {np.dtype(np.int32): 1, np.dtype(np.int64): 2, np.dtype(np.float64): 3}
+    with open(path, "wb") as f:
+        f.write(b"T3NSCAP1")
+        for name, arr in rec.items():
+            arr = np.ascontiguousarray(arr)
+            h = np.zeros(1, _HDR)
+            h["name"] = name.encode()
+            h["dtype"] = codes[arr.dtype]
+            h["count"] = arr.size
+            f.write(h.tobytes())
+            f.write(arr.tobytes())
