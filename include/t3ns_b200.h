@@ -149,6 +149,20 @@ int t3ns_davidson_device(t3ns_heff *h, double *result, double *energy,
                          const double *diagonal, t3ns_davidson_info *info,
                          void *stream);
 
+/* Davidson with a caller-supplied host matvec (any operator): the subspace
+ * algebra runs on the device, each new basis vector is handed to
+ * `matvec(in, out, ctx)` in host memory.  Same algorithm and return codes as
+ * t3ns_davidson_host. */
+int t3ns_davidson_callback(int64_t size, void (*matvec)(const double *, double *, void *),
+                           void *ctx, double *result, double *energy, int max_vecs,
+                           int keep_deflate, double tol, int max_its,
+                           const double *diagonal, t3ns_davidson_info *info);
+
+/* The diagonal preconditioner with Olsen correction on host buffers
+ * (reference davidson_diagonal_preconditioner, src/davidson.c:223-257). */
+int t3ns_precondition_host(int64_t size, const double *result, double theta,
+                           const double *diagonal, double *vec_t);
+
 const char *t3ns_last_error(void);
 
 /* Library build identification (git-independent). */

@@ -73,6 +73,7 @@ static int opt_capture_limit = 1000000;  /* number of captures          */
 static int opt_capture_stop;             /* exit after the last capture */
 static int opt_capture_nvec = 2;         /* seeded matvec pairs         */
 static int opt_capture_noeig;            /* skip Davidson in capture    */
+static const char *opt_schedule_lib;     /* drop-in whose schedule to dump */
 static int opt_step_counter;
 static int opt_captured;
 
@@ -309,12 +310,28 @@ static int capture_step(struct Heffdata *hd, double *guess, int size,
         free(y);
         fclose(cap_fp);
         cap_fp = NULL;
+        if (opt_schedule_lib) {
+                /* the product's schedule compiler on the same Heffdata, loaded
+                 * privately so it does not replace the reference symbols */
+                static int (*wr)(const struct Heffdata *, const char *);
+                if (!wr) {
+                        void *h = dlopen(opt_schedule_lib, RTLD_NOW | RTLD_LOCAL);
+                        if (!h) { fprintf(stderr, "%s\n", dlerror()); exit(EXIT_FAILURE); }
+                        wr = (int (*)(const struct Heffdata *, const char *))
+                                dlsym(h, "t3ns_dropin_schedule_write");
+                        if (!wr) { fprintf(stderr, "no t3ns_dropin_schedule_write\n"); exit(EXIT_FAILURE); }
+                }
+                char sp[4096];
+                snprintf(sp, sizeof sp, "%s/step_%03d.sched", opt_capture_dir, opt_step_counter);
+                if (wr(hd, sp) != 0) { fprintf(stderr, "schedule write failed\n"); exit(EXIT_FAILURE); }
+        }
         ++opt_captured;
         fprintf(stdout, "CAPTURED %s size %d blocks %d\n", path, size, st->nrblocks);
         fflush(stdout);
         return ret;
 }
 
+#ifndef T3NS_RUN_DROPIN
 int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
                       int keep_deflate, double tol, int max_its,
                       const double *diagonal,
@@ -352,6 +369,7 @@ int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
         ++opt_step_counter;
         return ret;
 }
+#endif
 
 /* ------------------------------------------------------------------ */
 
@@ -388,6 +406,7 @@ int main(int argc, char **argv)
                 else if (!strcmp(a, "--capture-nvec") && v) { opt_capture_nvec = atoi(v); ++i; }
                 else if (!strcmp(a, "--capture-stop")) { opt_capture_stop = 1; }
                 else if (!strcmp(a, "--capture-noeig")) { opt_capture_noeig = 1; }
+                else if (!strcmp(a, "--schedule-lib") && v) { opt_schedule_lib = v; ++i; }
                 else if (!strcmp(a, "--regime") && v) {
                         struct regime *r = &regs[nreg++];
                         memset(r, 0, sizeof *r);

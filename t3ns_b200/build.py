@@ -55,8 +55,29 @@ def build_engine(force: bool = False) -> str:
     return out
 
 
+REFERENCE_INCLUDE = os.environ.get("T3NS_REFERENCE_INCLUDE", "/root/reference/include")
+SHIM_INCLUDE = os.path.join(ROOT, "oracle", "shim")
+
+
+def build_dropin(force: bool = False):
+    """libt3ns_dropin.so: the reference entry points on top of the engine.
+    Compiled against the reference headers, whose struct layouts it must
+    match; skipped (returns None) when they are not available."""
+    if not os.path.isdir(REFERENCE_INCLUDE):
+        return None
+    engine = build_engine()
+    out = os.path.join(LIBDIR, "libt3ns_dropin.so")
+    src = os.path.join(CSRC, "dropin", "heff_dropin.c")
+    if force or _stale(out, [src, engine, os.path.join(INCLUDE, "t3ns_b200.h")]):
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu11", "-w", "-DMAX_SYMMETRIES=5",
+              "-DNDEBUG", "-I", REFERENCE_INCLUDE, "-I", SHIM_INCLUDE, "-I", INCLUDE,
+              "-o", out, src, "-L", LIBDIR, "-l:libt3ns_b200.so", "-Wl,-rpath,$ORIGIN",
+              "-lpthread"])
+    return out
+
+
 def build_all(force: bool = False):
-    return {"engine": build_engine(force)}
+    return {"engine": build_engine(force), "dropin": build_dropin(force)}
 
 
 if __name__ == "__main__":

@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cmath>
+#include <functional>
 #include <vector>
 
 #include "common.h"
@@ -194,6 +195,30 @@ ritz_kernel(const double *__restrict__ V, const double *__restrict__ VA, int64_t
                 for (int k = 0; k < 3; ++k) partials[blockIdx.x * 3 + k] = out[k];
 }
 
+// partials[b*3 + {1,2}] = {sum uK t, sum uK result} (the preconditioner's
+// reductions alone, for the standalone entry point)
+__global__ void __launch_bounds__(kRedThreads)
+precond_sums_kernel(const double *__restrict__ result, const double *__restrict__ t,
+                    const double *__restrict__ diag, const double *__restrict__ theta_p,
+                    int64_t n, double *__restrict__ partials)
+{
+        const double theta = *theta_p;
+        double acc[3] = {0, 0, 0};
+        for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+             i += (int64_t) gridDim.x * blockDim.x) {
+                const double r = result[i];
+                const double diff = diag[i] - theta;
+                const double uK = fabs(diff) > kDiagCutoff ? r / diff
+                                                           : (diff < 0 ? -1 : 1) * r / kDiagCutoff;
+                acc[1] = fma(uK, t[i], acc[1]);
+                acc[2] = fma(uK, r, acc[2]);
+        }
+        double out[3];
+        block_sums<3>(acc, out);
+        if (threadIdx.x == 0)
+                for (int k = 0; k < 3; ++k) partials[blockIdx.x * 3 + k] = out[k];
+}
+
 // t = -(t + alpha result) / (diag - theta) with alpha = -uKr / uKu
 __global__ void __launch_bounds__(kRedThreads)
 precond_kernel(const double *__restrict__ result, double *__restrict__ t,
@@ -270,7 +295,9 @@ __global__ void jacobi_eig_kernel(const double *__restrict__ S, int ld, int m,
                         frob_s = fr;
                 }
                 __syncthreads();
-                if (off_s <= 1e-32 * frob_s || off_s == 0.0) break;
+                // rounding keeps the off-diagonal norm near eps * m * ||A||;
+                // 1e-14 relative is below what the Ritz values can resolve
+                if (off_s <= 1e-28 * frob_s || off_s == 0.0) break;
                 for (int r = 0; r < M - 1; ++r) {
                         // round-robin pairing: player 0 fixed, others rotate
                         if (tid < M / 2) {
@@ -332,7 +359,7 @@ __global__ void jacobi_eig_kernel(const double *__restrict__ S, int ld, int m,
                         order[i] = order[best];
                         order[best] = tmp;
                 }
-                *status = sweep < max_sweeps ? 0 : 1;
+                *status = (sweep < max_sweeps || off_s <= 1e-20 * frob_s) ? 0 : 1;
         }
         __syncthreads();
         for (int e = tid; e < m * m; e += nt) {
@@ -378,12 +405,14 @@ static int alloc_basis(DavidsonBuffers &b, int64_t n, int max_vecs)
         return -1;
 }
 
-int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
-                 int keep, double tol, int max_its, const double *d_diag,
-                 t3ns_davidson_info *info, cudaStream_t s)
+// y = H x on device vectors, enqueued on the given stream
+using DevMatvec = std::function<int(const double *, double *, cudaStream_t)>;
+
+static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, double *energy,
+                         int max_vecs, int keep, double tol, int max_its, const double *d_diag,
+                         t3ns_davidson_info *info, cudaStream_t s)
 {
         const auto t_start = std::chrono::steady_clock::now();
-        const int64_t n = h->hp.size;
         if (max_vecs > kMaxVecs || keep > 4 || keep < 1 || keep >= max_vecs || max_vecs < 3)
                 return set_error(T3NS_E_LIMIT, "davidson: need 1 <= keep_deflate <= 4, "
                                                "keep_deflate < max_vecs <= 32");
@@ -435,8 +464,7 @@ int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
                 }
                 normalize_kernel<<<G, T, 0, s>>>(b.t, vm, n, b.partials, G);
                 T3NS_CUDA_TRY(cudaGetLastError());
-                int launches = 0;
-                T3NS_TRY(launch_heff_fp64(h->dp, vm, b.VA + (int64_t) m * n, s, &launches));
+                T3NS_TRY(matvec(vm, b.VA + (int64_t) m * n, s));
                 T3NS_TRY(column_of_S(m));
                 ++m;
                 T3NS_TRY(eigsolve(m));
@@ -486,6 +514,18 @@ int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
         return its >= max_its ? 1 : 0;
 }
 
+int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
+                 int keep, double tol, int max_its, const double *d_diag,
+                 t3ns_davidson_info *info, cudaStream_t s)
+{
+        DevMatvec mv = [h](const double *x, double *y, cudaStream_t st) {
+                int launches = 0;
+                return launch_heff_fp64(h->dp, x, y, st, &launches);
+        };
+        return davidson_core(h->hp.size, mv, d_result, energy, max_vecs, keep, tol, max_its,
+                             d_diag, info, s);
+}
+
 }  // namespace t3ns
 
 using namespace t3ns;
@@ -525,6 +565,83 @@ int t3ns_davidson_host(t3ns_heff *h, double *result, double *energy, int max_vec
                 rc = set_error(T3NS_E_CUDA, "davidson: download");
         cudaFree(d_res);
         cudaFree(d_diag);
+        return rc;
+}
+
+int t3ns_davidson_callback(int64_t size, void (*matvec)(const double *, double *, void *),
+                           void *ctx, double *result, double *energy, int max_vecs,
+                           int keep_deflate, double tol, int max_its, const double *diagonal,
+                           t3ns_davidson_info *info)
+{
+        if (!matvec || !result || !energy || !diagonal || size <= 0)
+                return set_error(T3NS_E_ARG, "null argument");
+        const size_t bytes = sizeof(double) * size;
+        double *d_res = nullptr, *d_diag = nullptr, *h_in = nullptr, *h_out = nullptr;
+        cudaStream_t s = nullptr;
+        int rc = T3NS_OK;
+        if (cudaMalloc(&d_res, bytes) != cudaSuccess || cudaMalloc(&d_diag, bytes) != cudaSuccess ||
+            cudaMallocHost(&h_in, bytes) != cudaSuccess || cudaMallocHost(&h_out, bytes) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+                cudaGetLastError();
+                rc = set_error(T3NS_E_NOMEM, "davidson: buffers");
+        }
+        if (rc == T3NS_OK &&
+            (cudaMemcpy(d_res, result, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+             cudaMemcpy(d_diag, diagonal, bytes, cudaMemcpyHostToDevice) != cudaSuccess))
+                rc = set_error(T3NS_E_CUDA, "davidson: upload");
+        if (rc == T3NS_OK) {
+                // the caller's matvec runs on the host: the new basis vector
+                // goes down, its image comes back up
+                DevMatvec mv = [&](const double *x, double *y, cudaStream_t st) {
+                        T3NS_CUDA_TRY(cudaMemcpyAsync(h_in, x, bytes, cudaMemcpyDeviceToHost, st));
+                        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
+                        matvec(h_in, h_out, ctx);
+                        T3NS_CUDA_TRY(cudaMemcpyAsync(y, h_out, bytes, cudaMemcpyHostToDevice, st));
+                        return T3NS_OK;
+                };
+                rc = davidson_core(size, mv, d_res, energy, max_vecs, keep_deflate, tol, max_its,
+                                   d_diag, info, s);
+        }
+        if (rc >= 0 && cudaMemcpy(result, d_res, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = set_error(T3NS_E_CUDA, "davidson: download");
+        if (s) cudaStreamDestroy(s);
+        cudaFree(d_res);
+        cudaFree(d_diag);
+        cudaFreeHost(h_in);
+        cudaFreeHost(h_out);
+        return rc;
+}
+
+int t3ns_precondition_host(int64_t size, const double *result, double theta,
+                           const double *diagonal, double *vec_t)
+{
+        if (!result || !diagonal || !vec_t || size <= 0) return set_error(T3NS_E_ARG, "null argument");
+        const size_t bytes = sizeof(double) * size;
+        double *d = nullptr;
+        double *scal = nullptr;
+        int rc = T3NS_OK;
+        if (cudaMalloc(&d, 3 * bytes + sizeof(double) * (kRedBlocks * 3 + 8)) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(T3NS_E_NOMEM, "precondition: buffers");
+        }
+        double *d_r = d, *d_diag = d + size, *d_t = d + 2 * size;
+        double *part = d + 3 * size;
+        scal = part + kRedBlocks * 3;
+        double *d_theta = scal + 4;
+        if (cudaMemcpy(d_r, result, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_diag, diagonal, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_t, vec_t, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_theta, &theta, sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = set_error(T3NS_E_CUDA, "precondition: upload");
+        if (rc == T3NS_OK) {
+                precond_sums_kernel<<<kRedBlocks, kRedThreads>>>(d_r, d_t, d_diag, d_theta, size, part);
+                reduce_partials_kernel<<<1, 64>>>(part, kRedBlocks, 3, scal, 1, 1.0);
+                precond_kernel<<<kRedBlocks, kRedThreads>>>(d_r, d_t, d_diag, scal, d_theta, size);
+                if (cudaGetLastError() != cudaSuccess ||
+                    cudaMemcpy(vec_t, d_t, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+                        rc = set_error(T3NS_E_CUDA, "precondition: kernels");
+        }
+        cudaFree(d);
         return rc;
 }
 
