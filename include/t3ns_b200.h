@@ -163,6 +163,11 @@ int t3ns_davidson_callback(int64_t size, void (*matvec)(const double *, double *
 int t3ns_precondition_host(int64_t size, const double *result, double theta,
                            const double *diagonal, double *vec_t);
 
+/* Diagnostic: builds the host-side plan of `desc` (no GPU needed) and writes
+ * its work units, pair sequences and flattened terms to `path` (step-file
+ * record layout), for host-side checks of the tiling and ordering. */
+int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path);
+
 const char *t3ns_last_error(void);
 
 /* Library build identification (git-independent). */

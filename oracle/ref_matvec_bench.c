@@ -9,9 +9,12 @@
  * exec_secondrun (src/Heff.c:945-1000) with OpenMP over new blocks and
  * OpenBLAS dgemm, exactly as inside the reference Davidson.
  *
- *   ref_matvec_bench STEPFILE [CALLS]
+ *   ref_matvec_bench STEPFILE [CALLS] [STRIDE]
  * prints one JSON line: seconds per matvec (median of CALLS), the algorithmic
  * FLOPs of the step, and the relative difference to the captured output.
+ * With STRIDE > 1 only every STRIDE-th new block keeps its schedule (a
+ * bounded sample of the step: the FLOPs reported are those of the kept
+ * blocks, and the output comparison is skipped).
  */
 #include <math.h>
 #include <stdint.h>
@@ -47,6 +50,13 @@ static void load(const char *path)
         fclose(f);
 }
 
+static void *find(const char *name)
+{
+        for (int i = 0; i < nrecs; ++i)
+                if (!strcmp(recs[i].name, name)) return recs[i].data;
+        return NULL;
+}
+
 static void *get(const char *name)
 {
         for (int i = 0; i < nrecs; ++i)
@@ -75,6 +85,7 @@ int main(int argc, char **argv)
         if (argc < 2) { fprintf(stderr, "usage: %s STEPFILE [CALLS]\n", argv[0]); return 2; }
         load(argv[1]);
         const int calls = argc > 2 ? atoi(argv[2]) : 3;
+        const int stride = argc > 3 ? atoi(argv[3]) : 1;
         struct Heffdata hd;
         memset(&hd, 0, sizeof hd);
         hd.isdmrg = geti("isdmrg");
@@ -100,7 +111,18 @@ int main(int argc, char **argv)
                 snprintf(nm, sizeof nm, "ops%d.beginblock", i);
                 int *bb = get(nm);
                 snprintf(nm, sizeof nm, "ops%d.tel", i);
-                double *tel = get(nm);
+                double *tel = find(nm);
+                if (!tel) {
+                        /* structure-only step file: any values do for timing */
+                        snprintf(nm, sizeof nm, "ops%d.tel_len", i);
+                        const int64_t n = *(int64_t *) get(nm);
+                        tel = malloc(sizeof *tel * (size_t) (n ? n : 1));
+                        uint64_t st = 2024u + (uint64_t) i;
+                        for (int64_t e = 0; e < n; ++e) {
+                                st = st * 6364136223846793005ull + 1442695040888963407ull;
+                                tel[e] = ((double) (st >> 11) * 0x1.0p-53 - 0.5) * 0.2;
+                        }
+                }
                 op->operators = calloc((size_t) op->nrops, sizeof *op->operators);
                 int64_t pb = 0, pt = 0;
                 for (int k = 0; k < op->nrops; ++k) {
@@ -139,7 +161,7 @@ int main(int argc, char **argv)
         double flops = 0;
         for (int i = 0; i < nb; ++i) {
                 for (int k = 0; k < 3; ++k) hd.sr.dimsofsb[i][k] = dims[3 * i + k];
-                hd.sr.nr_oldsb[i] = pptr[i + 1] - pptr[i];
+                hd.sr.nr_oldsb[i] = (i % stride == 0) ? pptr[i + 1] - pptr[i] : 0;
                 hd.sr.ntom[i] = malloc(sizeof **hd.sr.ntom * (size_t) (hd.sr.nr_oldsb[i] + 1));
                 for (int j = 0; j < hd.sr.nr_oldsb[i]; ++j) {
                         const int p = pptr[i] + j;
@@ -184,8 +206,12 @@ int main(int argc, char **argv)
         }
 
         const int size = hd.siteObject.blocks.beginblock[nb];
-        double *x = get("x1"), *yref = get("y1");
+        double *x = find("x1"), *yref = find("y1");
         double *y = malloc(sizeof *y * (size_t) size);
+        if (!x) {
+                x = malloc(sizeof *x * (size_t) size);
+                for (int i = 0; i < size; ++i) x[i] = 1.0 / sqrt((double) size);
+        }
         double *ts = malloc(sizeof *ts * (size_t) (calls > 0 ? calls : 1));
         for (int c = 0; c < calls; ++c) {
                 const double t0 = now();
@@ -193,13 +219,13 @@ int main(int argc, char **argv)
                 ts[c] = now() - t0;
         }
         double dn2 = 0, rn2 = 0;
-        for (int i = 0; i < size; ++i) {
+        for (int i = 0; i < size && stride == 1 && yref; ++i) {
                 dn2 += (y[i] - yref[i]) * (y[i] - yref[i]);
                 rn2 += yref[i] * yref[i];
         }
         qsort(ts, (size_t) calls, sizeof *ts, cmpd);
         printf("{\"seconds_per_matvec\": %.6e, \"calls\": %d, \"flops\": %.6e, "
-               "\"rel_diff_vs_capture\": %.3e, \"size\": %d}\n",
-               ts[calls / 2], calls, flops, sqrt(dn2 / (rn2 > 0 ? rn2 : 1)), size);
+               "\"rel_diff_vs_capture\": %.3e, \"size\": %d, \"stride\": %d}\n",
+               ts[calls / 2], calls, flops, sqrt(dn2 / (rn2 > 0 ? rn2 : 1)), size, stride);
         return 0;
 }

@@ -64,17 +64,17 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
         }
         T3NS_TRY(upload(h, &dp.blk_off, hp.block_off.data(), hp.block_off.size()));
         T3NS_TRY(upload(h, &dp.edims, hp.edims.data(), hp.edims.size()));
-        T3NS_TRY(upload(h, &dp.work_order, hp.work_order.data(), hp.work_order.size()));
-        dp.n_active = (int) hp.work_order.size();
         T3NS_TRY(upload(h, &dp.task_ptr, hp.task_ptr.data(), hp.task_ptr.size()));
         T3NS_TRY(upload(h, &dp.tasks, hp.tasks.data(), hp.tasks.size()));
+        T3NS_TRY(upload(h, &dp.pair_ptr, hp.pair_ptr.data(), hp.pair_ptr.size()));
+        T3NS_TRY(upload(h, &dp.pairs, hp.pairs.data(), hp.pairs.size()));
+        T3NS_TRY(upload(h, &dp.units, hp.units.data(), hp.units.size()));
+        dp.n_units = (int) hp.units.size();
+        T3NS_TRY(dev_alloc(h, &dp.counter, 1));
 
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-        dp.grid = std::max(1, std::min(dp.n_active, sms * 4));
-        dp.scratch_w1 = (hp.max_w1 + 31) / 32 * 32;
-        dp.scratch_w2 = (hp.max_w2 + 31) / 32 * 32;
-        T3NS_TRY(dev_alloc(h, &dp.scratch, (size_t) dp.grid * (dp.scratch_w1 + dp.scratch_w2)));
+        dp.grid = std::max(1, std::min(dp.n_units, 2 * sms));
         T3NS_TRY(dev_alloc(h, &dp.err, 1));
         T3NS_CUDA_TRY(cudaMemset(dp.err, 0, sizeof(int)));
         T3NS_TRY(dev_alloc(h, &h->stage_x, (size_t) hp.size));
@@ -172,8 +172,7 @@ int t3ns_heff_get_stats(const t3ns_heff *h, t3ns_heff_stats *st)
         st->flops_exec = h->hp.flops_exec;
         st->bytes_alg = h->hp.bytes_alg;
         st->op_elems = h->hp.op_elems;
-        st->scratch_bytes = (int64_t) sizeof(double) * h->dp.grid *
-                            (h->dp.scratch_w1 + h->dp.scratch_w2);
+        st->scratch_bytes = 0;
         return T3NS_OK;
 }
 
@@ -185,6 +184,43 @@ void t3ns_heff_destroy(t3ns_heff *h)
         if (h->stream) cudaStreamDestroy(h->stream);
         for (void *p : h->allocs) cudaFree(p);
         delete h;
+}
+
+int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path)
+{
+        HostPlan hp;
+        T3NS_TRY(build_plan(desc, hp));
+        FILE *f = fopen(path, "wb");
+        if (!f) return set_error(T3NS_E_ARG, std::string("cannot open ") + path);
+        auto put = [&](const char *name, int dtype, int64_t n, const void *a) {
+                char nm[48] = {0};
+                strncpy(nm, name, sizeof nm - 1);
+                int32_t hdr[2] = {dtype, 0};
+                fwrite(nm, 1, sizeof nm, f);
+                fwrite(hdr, sizeof hdr, 1, f);
+                fwrite(&n, sizeof n, 1, f);
+                if (n) fwrite(a, dtype == 1 ? 4 : 8, (size_t) n, f);
+        };
+        fwrite("T3NSCAP1", 1, 8, f);
+        std::vector<int> units, pairs, edims;
+        for (auto &u : hp.units) { units.insert(units.end(), {u.nb, u.b0, u.bt, u.c0, u.ct}); }
+        for (auto &p : hp.pairs) { pairs.insert(pairs.end(), {p.old, p.axes, p.t0, p.t1}); }
+        for (auto &e : hp.edims) { edims.insert(edims.end(), {e.x, e.y, e.z}); }
+        std::vector<int64_t> offs;
+        std::vector<double> prefs;
+        for (auto &t : hp.tasks) {
+                offs.insert(offs.end(), {t.op_off[0], t.op_off[1], t.op_off[2]});
+                prefs.push_back(t.pref);
+        }
+        put("plan.units", 1, (int64_t) units.size(), units.data());
+        put("plan.pairs", 1, (int64_t) pairs.size(), pairs.data());
+        put("plan.pair_ptr", 1, (int64_t) hp.pair_ptr.size(), hp.pair_ptr.data());
+        put("plan.edims", 1, (int64_t) edims.size(), edims.data());
+        put("plan.op_off", 2, (int64_t) offs.size(), offs.data());
+        put("plan.pref", 3, (int64_t) prefs.size(), prefs.data());
+        put("plan.flops", 3, 2, std::vector<double>{hp.flops_ref, hp.flops_exec}.data());
+        fclose(f);
+        return T3NS_OK;
 }
 
 const char *t3ns_last_error(void) { return g_last_error.c_str(); }

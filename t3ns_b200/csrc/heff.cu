@@ -8,18 +8,28 @@
 //
 // where X_i, Y_i, Z_i are the operator blocks acting on the three memory
 // axes of the block (memory axis j carries operator map[j]; reference
-// make_map, src/Heff.c:668-682) and each block is stored column-major with
-// the leg of axis 0 fastest.  The reference applies the three operators one
-// at a time with cblas_dgemm (do_contract, src/sparseblocks.c:133-158) in the
-// order chosen per (new, old) pair by make_cinfo (src/Heff.c:629-666).
+// make_map, src/Heff.c:668-682); blocks are column-major with axis 0
+// fastest and operator blocks are (new x old) column-major.  The reference
+// applies the three operators one at a time with cblas_dgemm (do_contract,
+// src/sparseblocks.c:133-158) in the order chosen per pair by make_cinfo
+// (src/Heff.c:629-666).
 //
-// Here the host flattens the schedule into one task per (pair, instruction)
-// whose three operator blocks are all present (find_operator_tel,
-// src/Heff.c:798-813), groups the tasks by output block, and one persistent
-// kernel walks them: each CTA owns whole output blocks (no atomics, as the
-// reference owns a new block per OpenMP thread) and runs the three
-// contractions of a task through shared-memory tiles, with the two
-// intermediates in a per-CTA scratch slice that stays resident in L2.
+// GPU organisation:
+//   * the host flattens the schedule into one term per (pair, instruction)
+//     whose three operator blocks are all present (find_operator_tel,
+//     src/Heff.c:798-813), grouped by pair, pairs grouped by output block;
+//   * an output block becomes one or more work units, tiles along memory
+//     axes 1 and 2 small enough for a shared-memory accumulator; a tiled
+//     block's pairs contract the tiled axes first, so a tile's share of the
+//     work is exactly its rows of the last operators (no recomputation);
+//   * one persistent kernel; each CTA takes units off a global counter
+//     (heaviest first), keeps the unit's output tile in shared memory and
+//     walks its pairs.  A pair's terms share every block dimension and the
+//     contraction order, so G terms at a time go through each stage as one
+//     uniform batched small GEMM with register micro-tiles; the stage before
+//     the last scales by the term prefactor, so the last stage is a plain
+//     reduction over the group inside each thread (single owner per output
+//     element: no atomics).
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -32,154 +42,210 @@
 
 namespace t3ns {
 
-// ---------------------------------------------------------------------------
-// CTA-wide FP64 GEMM on 64x64 output tiles, 256 threads, k-chunks of 16.
-//   C_l = alpha * A_l * op(B_l) + beta * C_l,  l < L, all column-major,
-//   op(B) = B (TB = false) or B^T (TB = true).
-// beta == 0 never reads C.  Every access is bounds-checked against M, N, K.
-template <bool TB>
-__device__ void cta_gemm(int M, int N, int K, int L,
-                         const double *__restrict__ A, int lda, int64_t sA,
-                         const double *__restrict__ B, int ldb, int64_t sB,
-                         double *C, int ldc, int64_t sC,
-                         double alpha, double beta, double (*As)[65], double (*Bs)[65])
+constexpr int kThreads = 256;
+constexpr int kOutCap = 2048;     // doubles: shared output tile
+constexpr int kPsiCap = 3072;     // doubles: staged old block (else read from L2)
+constexpr int kWCap = 6144;       // doubles: intermediates of a group
+constexpr int kGMax = 64;         // terms per group
+constexpr size_t kSmemBytes = sizeof(double) * (kOutCap + kPsiCap + kWCap + kGMax) +
+                              sizeof(int64_t) * 3 * kGMax + 64;
+
+// One contraction stage for G terms.  Term g applies rows [row0, row0+rows)
+// of the operator block at ops + opoff[g] (leading dimension ldop) on axis ax
+// of `in + g * in_gs` (dims w), writing `out + g * out_gs` (scaled by
+// scale[g] when scale != nullptr).  With ACC the G results are summed into
+// `out` instead (which then has no term stride).
+template <bool ACC>
+__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
+                                              const int64_t *opoff,
+                                              const double *__restrict__ ops, const double *in,
+                                              int in_gs, double *out, int out_gs,
+                                              const double *scale)
 {
+        int M, N, K, nc, ak, bk, bn, cn, a_cs, c_cs;
+        // A(m,k) = Ab[m + k*ak], B(k,n) = Bb[k*bk + n*bn], C(m,n) = Cb[m + n*cn]
+        if (ax == 0) {
+                M = rows; N = w[1] * w[2]; K = w[0]; nc = 1;
+                ak = ldop; bk = 1; bn = K; cn = rows; a_cs = 0; c_cs = 0;
+        } else if (ax == 1) {
+                M = w[0]; N = rows; K = w[1]; nc = w[2];
+                ak = w[0]; bk = ldop; bn = 1; cn = w[0];
+                a_cs = w[0] * w[1]; c_cs = w[0] * rows;
+        } else {
+                M = w[0] * w[1]; N = rows; K = w[2]; nc = 1;
+                ak = M; bk = ldop; bn = 1; cn = M; a_cs = 0; c_cs = 0;
+        }
+        const int mt = (M + 3) >> 2, nt = (N + 3) >> 2;
+        const int tiles = mt * nt;
+        const int gcn = (ACC ? 1 : G) * nc;
         const int tid = threadIdx.x;
-        const int tx = tid & 15, ty = tid >> 4;
-        const int tilesM = (M + 63) >> 6, tilesN = (N + 63) >> 6;
-        for (int l = 0; l < L; ++l) {
-                const double *Al = A + l * sA;
-                const double *Bl = B + l * sB;
-                double *Cl = C + l * sC;
-                for (int tile = 0; tile < tilesM * tilesN; ++tile) {
-                        const int m0 = (tile % tilesM) << 6;
-                        const int n0 = (tile / tilesM) << 6;
+        int tile0, tstep, gc0, gcstep;
+        if (tiles >= kThreads) {
+                tile0 = tid; tstep = kThreads; gc0 = 0; gcstep = 1;
+        } else {
+                const int nslot = kThreads / tiles;
+                const int slot = tid / tiles;
+                tile0 = slot < nslot ? tid - slot * tiles : tiles;
+                tstep = tiles;
+                gc0 = slot; gcstep = nslot;
+        }
+        for (int tile = tile0; tile < tiles; tile += tstep) {
+                const int tm = tile % mt, tn = tile / mt;
+                // interleaved micro-tile: rows tm + i*mt, columns tn + j*nt
+                for (int gc = gc0; gc < gcn; gc += gcstep) {
+                        const int c = ACC ? gc : gc % nc;
+                        const int g0 = ACC ? 0 : gc / nc;
+                        const int g1 = ACC ? G : g0 + 1;
                         double acc[4][4];
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
 #pragma unroll
                                 for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-                        for (int k0 = 0; k0 < K; k0 += 16) {
-#pragma unroll
-                                for (int r = 0; r < 4; ++r) {
-                                        const int e = tid + 256 * r;
-                                        const int m = e & 63, k = e >> 6;
-                                        const int gm = m0 + m, gk = k0 + k;
-                                        As[k][m] = (gm < M && gk < K)
-                                                ? Al[gm + (int64_t) gk * lda] : 0.0;
-                                }
-#pragma unroll
-                                for (int r = 0; r < 4; ++r) {
-                                        const int e = tid + 256 * r;
-                                        int n, k;
-                                        if (TB) { n = e & 63; k = e >> 6; }
-                                        else { k = e & 15; n = e >> 4; }
-                                        const int gn = n0 + n, gk = k0 + k;
-                                        double v = 0.0;
-                                        if (gn < N && gk < K)
-                                                v = TB ? Bl[gn + (int64_t) gk * ldb]
-                                                       : Bl[gk + (int64_t) gn * ldb];
-                                        Bs[k][n] = v;
-                                }
-                                __syncthreads();
-#pragma unroll
-                                for (int k = 0; k < 16; ++k) {
+                        for (int g = g0; g < g1; ++g) {
+                                const double *op = ops + opoff[g];
+                                const double *tin = in + g * in_gs;
+                                const double *Ab = ax == 0 ? op : tin + c * a_cs;
+                                const double *Bb = ax == 0 ? tin : op;
+                                for (int k = 0; k < K; ++k) {
                                         double a[4], b[4];
 #pragma unroll
-                                        for (int i = 0; i < 4; ++i) a[i] = As[k][tx + 16 * i];
+                                        for (int i = 0; i < 4; ++i) {
+                                                const int m = tm + i * mt;
+                                                a[i] = m < M ? Ab[m + k * ak] : 0.0;
+                                        }
 #pragma unroll
-                                        for (int j = 0; j < 4; ++j) b[j] = Bs[k][ty + 16 * j];
+                                        for (int j = 0; j < 4; ++j) {
+                                                const int n = tn + j * nt;
+                                                b[j] = n < N ? Bb[k * bk + n * bn] : 0.0;
+                                        }
 #pragma unroll
                                         for (int i = 0; i < 4; ++i)
 #pragma unroll
                                                 for (int j = 0; j < 4; ++j)
                                                         acc[i][j] = fma(a[i], b[j], acc[i][j]);
                                 }
-                                __syncthreads();
                         }
+                        const double sc = (!ACC && scale) ? scale[g0] : 1.0;
+                        double *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs;
 #pragma unroll
                         for (int i = 0; i < 4; ++i) {
-                                const int m = m0 + tx + 16 * i;
+                                const int m = tm + i * mt;
                                 if (m >= M) continue;
 #pragma unroll
                                 for (int j = 0; j < 4; ++j) {
-                                        const int n = n0 + ty + 16 * j;
+                                        const int n = tn + j * nt;
                                         if (n >= N) continue;
-                                        double *c = Cl + m + (int64_t) n * ldc;
-                                        const double v = alpha * acc[i][j];
-                                        *c = beta == 0.0 ? v : fma(beta, *c, v);
+                                        double *cp = Cb + m + n * cn;
+                                        *cp = ACC ? *cp + acc[i][j] : sc * acc[i][j];
                                 }
                         }
                 }
         }
 }
 
-// Applies the (r x s) operator block `op` on memory axis `ax` of the tensor
-// `in` with dims d[3] (d[ax] == s), writing `out` with d[ax] replaced by r.
-__device__ void apply_axis(int ax, const int *d, int r, const double *op,
-                           const double *in, double *out, double alpha, double beta,
-                           double (*As)[65], double (*Bs)[65])
-{
-        if (ax == 0) {
-                // out(r, d1 d2) = op(r x d0) * in(d0 x d1 d2)
-                cta_gemm<false>(r, d[1] * d[2], d[0], 1, op, r, 0, in, d[0], 0,
-                                out, r, 0, alpha, beta, As, Bs);
-        } else if (ax == 1) {
-                // out_l(d0 x r) = in_l(d0 x d1) * op^T, l < d2
-                cta_gemm<true>(d[0], r, d[1], d[2], in, d[0], (int64_t) d[0] * d[1],
-                               op, r, 0, out, d[0], (int64_t) d[0] * r,
-                               alpha, beta, As, Bs);
-        } else {
-                // out(d0 d1 x r) = in(d0 d1 x d2) * op^T
-                cta_gemm<true>(d[0] * d[1], r, d[2], 1, in, d[0] * d[1], 0,
-                               op, r, 0, out, d[0] * d[1], 0, alpha, beta, As, Bs);
-        }
-}
-
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kThreads, 2)
 heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                  const double *__restrict__ ops, const int64_t *__restrict__ blk_off,
-                 const int4 *__restrict__ edims, const int *__restrict__ work_order,
-                 int n_active, const int *__restrict__ task_ptr,
-                 const HeffTask *__restrict__ tasks, double *scratch,
-                 int64_t scratch_w1, int64_t scratch_w2, int *err)
+                 const int4 *__restrict__ edims, const HeffUnit *__restrict__ units, int n_units,
+                 const int *__restrict__ pair_ptr, const HeffPair *__restrict__ pairs,
+                 const HeffTask *__restrict__ tasks, int *counter, int *err)
 {
-        __shared__ double As[16][65];
-        __shared__ double Bs[16][65];
-        double *W1 = scratch + (int64_t) blockIdx.x * (scratch_w1 + scratch_w2);
-        double *W2 = W1 + scratch_w1;
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        double *OUT = reinterpret_cast<double *>(smem_raw);
+        double *PSI = OUT + kOutCap;
+        double *W = PSI + kPsiCap;
+        double *PREF = W + kWCap;
+        int64_t *OPOFF = reinterpret_cast<int64_t *>(PREF + kGMax);   // [3][kGMax]
+        int *UNIT = reinterpret_cast<int *>(OPOFF + 3 * kGMax);
+        const int tid = threadIdx.x;
 
-        for (int idx = blockIdx.x; idx < n_active; idx += gridDim.x) {
-                const int nb = work_order[idx];
+        for (;;) {
+                if (tid == 0) *UNIT = atomicAdd(counter, 1);
+                __syncthreads();
+                const int u = *UNIT;
+                __syncthreads();
+                if (u >= n_units) break;
+                const HeffUnit un = units[u];
+                const int nb = un.nb;
                 const int4 en = edims[nb];
                 const int dn[3] = {en.x, en.y, en.z};
-                double *yn = y + blk_off[nb];
-                for (int t = task_ptr[nb]; t < task_ptr[nb + 1]; ++t) {
-                        const HeffTask tk = tasks[t];
-                        const int4 eo = edims[tk.old];
-                        int w[3] = {eo.x, eo.y, eo.z};
-                        const double *in = x + blk_off[tk.old];
-                        const int nst = (tk.axes >> 6) & 3;
-                        for (int s = 0; s < nst; ++s) {
-                                const int ax = (tk.axes >> (2 * s)) & 3;
-                                const bool last = s == nst - 1;
-                                double *out = last ? yn : (s == 0 ? W1 : W2);
-                                const int64_t outsz = (int64_t) w[0] * w[1] * w[2] / w[ax] * dn[ax];
-                                if (!last && outsz > (s == 0 ? scratch_w1 : scratch_w2)) {
-                                        if (threadIdx.x == 0) atomicExch(err, 1);
-                                        return;
+                // extent and first row of the tile along each axis
+                const int ext[3] = {dn[0], un.bt, un.ct};
+                const int row0[3] = {0, un.b0, un.c0};
+                const int st = ext[0] * ext[1] * ext[2];
+                for (int e = tid; e < st; e += kThreads) OUT[e] = 0.0;
+                __syncthreads();
+                for (int p = pair_ptr[nb]; p < pair_ptr[nb + 1]; ++p) {
+                        const HeffPair pr = pairs[p];
+                        const int4 eo = edims[pr.old];
+                        const int nst = (pr.axes >> 6) & 3;
+                        int ax[3];
+                        for (int s = 0; s < 3; ++s) ax[s] = (pr.axes >> (2 * s)) & 3;
+                        const int w0[3] = {eo.x, eo.y, eo.z};
+                        int w1[3] = {w0[0], w0[1], w0[2]};
+                        w1[ax[0]] = ext[ax[0]];
+                        int w2[3] = {w1[0], w1[1], w1[2]};
+                        w2[ax[1]] = ext[ax[1]];
+                        const int s0 = w0[0] * w0[1] * w0[2];
+                        const int s1 = w1[0] * w1[1] * w1[2];
+                        const int s2 = nst == 3 ? w2[0] * w2[1] * w2[2] : 0;
+                        if (s1 + s2 > kWCap) {
+                                if (tid == 0) atomicExch(err, 3);
+                                return;
+                        }
+                        const double *xin = x + blk_off[pr.old];
+                        const double *in0 = xin;
+                        if (s0 <= kPsiCap) {
+                                for (int e = tid; e < s0; e += kThreads) PSI[e] = xin[e];
+                                in0 = PSI;
+                        }
+                        const int G = min(kGMax, kWCap / (s1 + s2));
+                        double *W1 = W, *W2 = W + G * s1;
+                        const int nterm = pr.t1 - pr.t0;
+                        for (int t0 = 0; t0 < nterm; t0 += G) {
+                                const int g = min(G, nterm - t0);
+                                if (tid < g) {
+                                        const HeffTask &tk = tasks[pr.t0 + t0 + tid];
+                                        for (int s = 0; s < 3; ++s)
+                                                OPOFF[s * kGMax + tid] = tk.op_off[ax[s]] + row0[ax[s]];
+                                        PREF[tid] = tk.pref;
                                 }
-                                apply_axis(ax, w, dn[ax], ops + tk.op_off[ax], in, out,
-                                           last ? tk.pref : 1.0, last ? 1.0 : 0.0, As, Bs);
                                 __syncthreads();
-                                w[ax] = dn[ax];
-                                in = out;
+                                if (nst == 3) {
+                                        grouped_stage<false>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
+                                                             ops, in0, 0, W1, s1, nullptr);
+                                        __syncthreads();
+                                        grouped_stage<false>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
+                                                             OPOFF + kGMax, ops, W1, s1, W2, s2, PREF);
+                                        __syncthreads();
+                                        grouped_stage<true>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
+                                                            OPOFF + 2 * kGMax, ops, W2, s2, OUT, 0,
+                                                            nullptr);
+                                } else {
+                                        grouped_stage<false>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
+                                                             ops, in0, 0, W1, s1, PREF);
+                                        __syncthreads();
+                                        grouped_stage<true>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
+                                                            OPOFF + kGMax, ops, W1, s1, OUT, 0,
+                                                            nullptr);
+                                }
+                                __syncthreads();
                         }
                 }
+                // write the tile back
+                double *yn = y + blk_off[nb];
+                for (int e = tid; e < st; e += kThreads) {
+                        const int a = e % ext[0];
+                        const int t = e / ext[0];
+                        const int b = t % ext[1];
+                        const int c = t / ext[1];
+                        yn[a + (int64_t) dn[0] * ((row0[1] + b) + (int64_t) dn[1] * (row0[2] + c))] = OUT[e];
+                }
+                __syncthreads();
         }
 }
 
-// Diagonal: diag[n](a,b,c) = sum over tasks of the (n, n) pair of
+// Diagonal: diag[n](a,b,c) = sum over the terms of the (n, n) pair of
 // pref * X[a,a] * Y[b,b] * Z[c,c]  (reference diag_old_to_new_sb,
 // src/Heff.c:1064-1108).
 __global__ void heff_diag_kernel(double *__restrict__ diag, const double *__restrict__ ops,
@@ -218,6 +284,58 @@ static const int kOrders3[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1},
                                    {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
 static const int kOrders2[2][2] = {{0, 1}, {1, 0}};
 
+// FLOPs of one term contracting axes in `seq` (memory axes) from dims `o`
+// to dims `n`, and the sizes of its first two intermediates for the tile
+// extents `ext` (equal to n on untiled axes).
+static double seq_cost(const int *seq, int nst, const int *o, const int *n, const int *ext,
+                       int64_t *s1, int64_t *s2)
+{
+        double fl = 0;
+        int64_t w[3] = {o[0], o[1], o[2]}, wt[3] = {o[0], o[1], o[2]};
+        for (int s = 0; s < nst; ++s) {
+                fl += 2.0 * (double) w[0] * w[1] * w[2] * n[seq[s]];
+                w[seq[s]] = n[seq[s]];
+                wt[seq[s]] = ext[seq[s]];
+                if (s == 0) *s1 = wt[0] * wt[1] * wt[2];
+                if (s == 1) *s2 = nst == 3 ? wt[0] * wt[1] * wt[2] : 0;
+        }
+        return fl;
+}
+
+// Cheapest contraction sequence for a pair whose first stages must be the
+// tiled axes (mask bit j: axis j is tiled), among those whose intermediates
+// fit the shared buffer.  Returns -1 if none fits.
+static int choose_seq(int nst, int tiled_mask, const int *o, const int *n, const int *ext,
+                      double *fl_out, int seq_out[3])
+{
+        static const int perms3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
+                                         {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+        static const int perms2[2][3] = {{0, 1, 2}, {1, 0, 2}};
+        const int np = nst == 3 ? 6 : 2;
+        int best = -1;
+        double bfl = 0;
+        for (int q = 0; q < np; ++q) {
+                const int *seq = nst == 3 ? perms3[q] : perms2[q];
+                // tiled axes must come before every untiled axis
+                bool ok = true, seen_untiled = false;
+                for (int s = 0; s < nst; ++s) {
+                        const bool t = (tiled_mask >> seq[s]) & 1;
+                        if (t && seen_untiled) ok = false;
+                        if (!t) seen_untiled = true;
+                }
+                if (!ok) continue;
+                int64_t s1 = 0, s2 = 0;
+                const double fl = seq_cost(seq, nst, o, n, ext, &s1, &s2);
+                if (s1 + s2 > kWCap) continue;
+                if (best < 0 || fl < bfl) { best = q; bfl = fl; }
+        }
+        if (best < 0) return -1;
+        const int *seq = nst == 3 ? perms3[best] : perms2[best];
+        for (int s = 0; s < 3; ++s) seq_out[s] = seq[s];
+        *fl_out = bfl;
+        return 0;
+}
+
 int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
 {
         if (!d || d->nblocks < 0) return set_error(T3NS_E_ARG, "null descriptor");
@@ -244,6 +362,8 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 if ((int64_t) e[0] * e[1] * e[2] != d->block_off[b + 1] - d->block_off[b])
                         return set_error(T3NS_E_ARG, "block size != product of dims at block " +
                                                           std::to_string(b));
+                if (e[0] > kOutCap)
+                        return set_error(T3NS_E_LIMIT, "leg dimension beyond the output tile");
                 hp.edims[b] = make_int4(e[0], e[1], e[2], 0);
         }
         hp.size = d->block_off[d->nblocks];
@@ -261,17 +381,24 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
         }
         hp.op_elems = tot;
 
-        // tasks
+        // terms, grouped by pair, pairs by new block
         hp.task_ptr.assign(d->nblocks + 1, 0);
+        hp.pair_ptr.assign(d->nblocks + 1, 0);
         hp.tasks.clear();
-        std::vector<double> work(d->nblocks, 0.0);
-        std::vector<char> seen_block;
-        double flops = 0;
-        int64_t npairs = 0, max_w1 = 0, max_w2 = 0;
+        hp.pairs.clear();
+        hp.units.clear();
+        double flops_ref = 0, flops_exec = 0;
+        int64_t npairs = 0;
+        std::vector<double> unit_work;
         for (int nb = 0; nb < d->nblocks; ++nb) {
                 hp.task_ptr[nb] = (int) hp.tasks.size();
+                hp.pair_ptr[nb] = (int) hp.pairs.size();
                 const int dn[3] = {d->dims[3 * nb], d->dims[3 * nb + 1],
                                    d->isdmrg ? 1 : d->dims[3 * nb + 2]};
+                const int4 en4 = hp.edims[nb];
+                const int en[3] = {en4.x, en4.y, en4.z};
+                struct PairTmp { int ob; int t0, t1; int eo[3]; };
+                std::vector<PairTmp> ptmp;
                 for (int p = d->pair_ptr[nb]; p < d->pair_ptr[nb + 1]; ++p) {
                         ++npairs;
                         const int ob = d->pair_old[p];
@@ -285,20 +412,14 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         const int *o = d->isdmrg ? kOrders2[ord] : kOrders3[ord];
                         // reference FLOP count of one instruction for this pair
                         double fl = 0;
-                        int wd[3] = {dold[0], dold[1], dold[2]};
-                        int64_t w1 = 0, w2 = 0;
-                        for (int s = 0; s < nops; ++s) {
-                                fl += (double) wd[0] * wd[1] * wd[2] * dn[o[s]];
-                                wd[o[s]] = dn[o[s]];
-                                const int64_t sz = (int64_t) wd[0] * wd[1] * wd[2];
-                                if (s == 0) w1 = sz;
-                                if (s == 1 && nops == 3) w2 = sz;
+                        {
+                                double wd[3] = {(double) dold[0], (double) dold[1], (double) dold[2]};
+                                for (int s = 0; s < nops; ++s) {
+                                        fl += 2.0 * wd[0] * wd[1] * wd[2] * dn[o[s]];
+                                        wd[o[s]] = dn[o[s]];
+                                }
                         }
-                        int axes = 0;
-                        for (int s = 0; s < nops; ++s) axes |= inv_map[o[s]] << (2 * s);
-                        if (d->isdmrg) { axes = 0; for (int s = 0; s < 2; ++s) axes |= o[s] << (2 * s); }
-                        axes |= nops << 6;
-
+                        const int t0 = (int) hp.tasks.size();
                         for (int64_t c = d->combo_ptr[p]; c < d->combo_ptr[p + 1]; ++c) {
                                 const int m = d->combo_mpo[c];
                                 if (m < 0 || m >= d->nrMPOc)
@@ -327,31 +448,94 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                         if (!present) continue;
                                         t.pref = d->instr_pref[k] * d->combo_pref[c];
                                         t.old = ob;
-                                        t.axes = axes;
+                                        t.axes = nops << 6;
                                         hp.tasks.push_back(t);
-                                        flops += 2.0 * fl;
-                                        work[nb] += 2.0 * fl + 64.0;
-                                        max_w1 = std::max(max_w1, w1);
-                                        max_w2 = std::max(max_w2, w2);
+                                        flops_ref += fl;
                                 }
                         }
+                        const int t1 = (int) hp.tasks.size();
+                        if (t1 > t0) {
+                                const int4 eo4 = hp.edims[ob];
+                                ptmp.push_back({ob, t0, t1, {eo4.x, eo4.y, eo4.z}});
+                        }
                 }
+                if (ptmp.empty()) continue;
+
+                // tiling of the output block and a sequence per pair that fits
+                const int64_t sn = (int64_t) en[0] * en[1] * en[2];
+                std::vector<std::pair<int, int>> cand;   // (bt, ct)
+                if (sn <= kOutCap) cand.push_back({en[1], en[2]});
+                if ((int64_t) en[0] * en[1] <= kOutCap)
+                        for (int ct = (int) std::min<int64_t>(en[2], kOutCap / ((int64_t) en[0] * en[1]));
+                             ct >= 1; ct = ct / 2)
+                                cand.push_back({en[1], ct});
+                for (int bt = std::min(en[1], kOutCap / en[0]); bt >= 1; bt = bt / 2)
+                        cand.push_back({bt, 1});
+                bool placed = false;
+                for (auto [bt, ct] : cand) {
+                        const int mask = (bt < en[1] ? 2 : 0) | (ct < en[2] ? 4 : 0);
+                        const int ext[3] = {en[0], bt, ct};
+                        std::vector<int> seqs(ptmp.size());
+                        double fl_blk = 0;
+                        bool ok = true;
+                        for (size_t q = 0; q < ptmp.size() && ok; ++q) {
+                                int seq[3];
+                                double fl;
+                                if (choose_seq(nops, mask, ptmp[q].eo, en, ext, &fl, seq) != 0) {
+                                        ok = false;
+                                        break;
+                                }
+                                int axes = nops << 6;
+                                for (int s = 0; s < nops; ++s) axes |= seq[s] << (2 * s);
+                                seqs[q] = axes;
+                                fl_blk += fl * (ptmp[q].t1 - ptmp[q].t0);
+                        }
+                        if (!ok) continue;
+                        for (size_t q = 0; q < ptmp.size(); ++q)
+                                hp.pairs.push_back({ptmp[q].ob, seqs[q], ptmp[q].t0, ptmp[q].t1});
+                        flops_exec += fl_blk;
+                        const int nbt = (en[1] + bt - 1) / bt, nct = (en[2] + ct - 1) / ct;
+                        for (int ib = 0; ib < nbt; ++ib)
+                                for (int ic = 0; ic < nct; ++ic) {
+                                        HeffUnit u{};
+                                        u.nb = nb;
+                                        u.b0 = ib * bt;
+                                        u.bt = std::min(bt, en[1] - u.b0);
+                                        u.c0 = ic * ct;
+                                        u.ct = std::min(ct, en[2] - u.c0);
+                                        hp.units.push_back(u);
+                                        unit_work.push_back(fl_blk * u.bt * u.ct /
+                                                            ((double) en[1] * en[2]) +
+                                                            1e4 * ptmp.size());
+                                }
+                        placed = true;
+                        break;
+                }
+                if (!placed)
+                        return set_error(T3NS_E_LIMIT, "no tiling of output block " + std::to_string(nb) +
+                                                               " fits the shared-memory buffers");
         }
         hp.task_ptr[d->nblocks] = (int) hp.tasks.size();
+        hp.pair_ptr[d->nblocks] = (int) hp.pairs.size();
         if (hp.tasks.size() > (size_t) INT32_MAX)
                 return set_error(T3NS_E_LIMIT, "more than 2^31 tasks");
         hp.npairs = npairs;
-        hp.flops_ref = flops;
-        hp.flops_exec = flops;
-        hp.max_w1 = max_w1;
-        hp.max_w2 = max_w2;
+        hp.flops_ref = flops_ref;
+        hp.flops_exec = flops_exec;
+
+        // heaviest units first
+        std::vector<int> idx(hp.units.size());
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(),
+                         [&](int a, int b) { return unit_work[a] > unit_work[b]; });
+        std::vector<HeffUnit> sorted(hp.units.size());
+        for (size_t i = 0; i < idx.size(); ++i) sorted[i] = hp.units[idx[i]];
+        hp.units.swap(sorted);
 
         // algorithmic bytes: vectors in/out + each referenced operator block once
         {
-                std::vector<int64_t> offs;
-                offs.reserve(hp.tasks.size() * 3);
-                double opbytes = 0;
                 std::vector<std::pair<int64_t, int64_t>> blocks;
+                blocks.reserve(hp.tasks.size() * nops);
                 for (int nb = 0; nb < d->nblocks; ++nb)
                         for (int t = hp.task_ptr[nb]; t < hp.task_ptr[nb + 1]; ++t) {
                                 const HeffTask &tk = hp.tasks[t];
@@ -362,16 +546,10 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         }
                 std::sort(blocks.begin(), blocks.end());
                 blocks.erase(std::unique(blocks.begin(), blocks.end()), blocks.end());
+                double opbytes = 0;
                 for (auto &b : blocks) opbytes += 8.0 * b.second;
                 hp.bytes_alg = 16.0 * hp.size + opbytes;
         }
-
-        // active output blocks, heaviest first (longest-processing-time order)
-        hp.work_order.clear();
-        for (int nb = 0; nb < d->nblocks; ++nb)
-                if (hp.task_ptr[nb + 1] > hp.task_ptr[nb]) hp.work_order.push_back(nb);
-        std::stable_sort(hp.work_order.begin(), hp.work_order.end(),
-                         [&](int a, int b) { return work[a] > work[b]; });
         return T3NS_OK;
 }
 
@@ -379,11 +557,18 @@ int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStrea
                      int *launches)
 {
         T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
-        if (dp.n_active > 0) {
-                heff_fp64_kernel<<<dp.grid, 256, 0, s>>>(
-                        x, y, dp.ops, dp.blk_off, dp.edims, dp.work_order, dp.n_active,
-                        dp.task_ptr, dp.tasks, dp.scratch, dp.scratch_w1, dp.scratch_w2,
-                        dp.err);
+        if (dp.n_units > 0) {
+                static bool attr_set = false;
+                if (!attr_set) {
+                        T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_fp64_kernel,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           (int) kSmemBytes));
+                        attr_set = true;
+                }
+                T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
+                heff_fp64_kernel<<<dp.grid, kThreads, kSmemBytes, s>>>(
+                        x, y, dp.ops, dp.blk_off, dp.edims, dp.units, dp.n_units, dp.pair_ptr,
+                        dp.pairs, dp.tasks, dp.counter, dp.err);
                 T3NS_CUDA_TRY(cudaGetLastError());
                 if (launches) *launches = 1;
         } else if (launches) {

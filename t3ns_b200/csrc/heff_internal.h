@@ -19,6 +19,23 @@ struct __align__(16) HeffTask {
         int axes;
 };
 
+// One (new, old) block pair: its terms are tasks[t0, t1); `axes` packs the
+// contraction sequence chosen for the pair (same encoding as HeffTask).
+struct __align__(16) HeffPair {
+        int old;
+        int axes;
+        int t0, t1;
+};
+
+// One unit of kernel work: the output tile [0,d0) x [b0,b0+bt) x [c0,c0+ct)
+// of new block nb (memory axes), with all of nb's pairs.
+struct __align__(16) HeffUnit {
+        int nb;
+        int b0, bt;
+        int c0, ct;
+        int pad[3];
+};
+
 struct HostPlan {
         int isdmrg = 0;
         int map[3] = {0, 1, 2};
@@ -30,9 +47,11 @@ struct HostPlan {
         int64_t op_elems = 0;
         std::vector<int> task_ptr;
         std::vector<HeffTask> tasks;
+        std::vector<int> pair_ptr;                // [nblocks + 1] into pairs
+        std::vector<HeffPair> pairs;
         std::vector<int> work_order;
+        std::vector<HeffUnit> units;              // heaviest first
         int64_t npairs = 0;
-        int64_t max_w1 = 0, max_w2 = 0;
         double flops_ref = 0, flops_exec = 0, bytes_alg = 0;
 };
 
@@ -46,8 +65,11 @@ struct DevicePlan {
         int n_active = 0;
         int *task_ptr = nullptr;
         HeffTask *tasks = nullptr;
-        double *scratch = nullptr;
-        int64_t scratch_w1 = 0, scratch_w2 = 0;
+        int *pair_ptr = nullptr;
+        HeffPair *pairs = nullptr;
+        HeffUnit *units = nullptr;
+        int n_units = 0;
+        int *counter = nullptr;                   // dynamic unit scheduler
         int grid = 0;
         int *err = nullptr;
 };

@@ -21,8 +21,16 @@ _DTYPES = {1: np.int32, 2: np.int64, 3: np.float64}
 _HDR = np.dtype([("name", "S48"), ("dtype", "<i4"), ("pad", "<i4"), ("count", "<i8")])
 
 
+def synthesize_operator_values(n: int, opset: int) -> np.ndarray:
+    """Operator elements of a structure-only step file: N(0, 0.1^2) from the
+    fixed seed 2024 + opset (numpy PCG64)."""
+    return np.random.default_rng(2024 + opset).standard_normal(n) * 0.1
+
+
 def read_step(path) -> dict:
-    """Return ``{name: ndarray}`` for every record of a step file."""
+    """Return ``{name: ndarray}`` for every record of a step file.  For a
+    structure-only file (``ops{i}.tel_len`` instead of ``ops{i}.tel``) the
+    operator elements are synthesized (``synthesize_operator_values``)."""
     with open(path, "rb") as f:
         buf = f.read()
     if buf[:8] != b"T3NSCAP1":
@@ -37,6 +45,9 @@ def read_step(path) -> dict:
         arr = np.frombuffer(buf, dt, n, pos).copy()
         pos += n * dt.itemsize
         out[hdr["name"].decode()] = arr
+    for i in range(3):
+        if f"ops{i}.tel_len" in out and f"ops{i}.tel" not in out:
+            out[f"ops{i}.tel"] = synthesize_operator_values(int(out[f"ops{i}.tel_len"][0]), i)
     return out
 
 
