@@ -203,7 +203,7 @@ int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path)
         };
         fwrite("T3NSCAP1", 1, 8, f);
         std::vector<int> units, pairs, edims;
-        for (auto &u : hp.units) { units.insert(units.end(), {u.nb, u.b0, u.bt, u.c0, u.ct}); }
+        for (auto &u : hp.units) { units.insert(units.end(), {u.nb, u.b0, u.bt, u.c0, u.ct, u.a0, u.at, u.p0, u.p1, u.split}); }
         for (auto &p : hp.pairs) { pairs.insert(pairs.end(), {p.old, p.axes, p.t0, p.t1}); }
         for (auto &e : hp.edims) { edims.insert(edims.end(), {e.x, e.y, e.z}); }
         std::vector<int64_t> offs;

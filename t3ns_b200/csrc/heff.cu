@@ -26,11 +26,13 @@
 //     (heaviest first), keeps the unit's output tile in shared memory and
 //     walks its pairs.  A pair's terms share every block dimension and the
 //     contraction order, so G terms at a time go through each stage as one
-//     uniform batched small GEMM with register micro-tiles; the stage before
+//     uniform batched small GEMM on the FP64 tensor pipe (mma.m8n8k4, one
+//     8x8 output tile per warp at a time); the stage before
 //     the last scales by the term prefactor, so the last stage is a plain
-//     reduction over the group inside each thread (single owner per output
+//     reduction over the group inside each warp (single owner per output
 //     element: no atomics).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -45,16 +47,29 @@ namespace t3ns {
 constexpr int kThreads = 256;
 constexpr int kOutCap = 2048;     // doubles: shared output tile
 constexpr int kPsiCap = 3072;     // doubles: staged old block (else read from L2)
-constexpr int kWCap = 6144;       // doubles: intermediates of a group
+constexpr int kWCap = 8192;       // doubles: intermediates of a group
 constexpr int kGMax = 64;         // terms per group
+constexpr double kPairVisitCost = 4e4;   // FLOP-equivalent of one (unit, pair) visit
 constexpr size_t kSmemBytes = sizeof(double) * (kOutCap + kPsiCap + kWCap + kGMax) +
                               sizeof(int64_t) * 3 * kGMax + 64;
+
+// D(8x8) += A(8x4) * B(4x8) on the FP64 tensor pipe (one warp).  Fragment
+// layout (PTX ISA, mma.m8n8k4 .f64): lane l holds A[l/4][l%4], B[l%4][l/4]
+// and D[l/4][2*(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+{
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                     : "+d"(d0), "+d"(d1)
+                     : "d"(a), "d"(b));
+}
 
 // One contraction stage for G terms.  Term g applies rows [row0, row0+rows)
 // of the operator block at ops + opoff[g] (leading dimension ldop) on axis ax
 // of `in + g * in_gs` (dims w), writing `out + g * out_gs` (scaled by
 // scale[g] when scale != nullptr).  With ACC the G results are summed into
-// `out` instead (which then has no term stride).
+// `out` instead (which then has no term stride).  Each warp owns 8x8 output
+// tiles and runs their K loop on the FP64 tensor pipe; with ACC the group
+// reduction stays inside the warp's accumulators.
 template <bool ACC>
 __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
                                               const int64_t *opoff,
@@ -75,69 +90,62 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                 M = w[0] * w[1]; N = rows; K = w[2]; nc = 1;
                 ak = M; bk = ldop; bn = 1; cn = M; a_cs = 0; c_cs = 0;
         }
-        const int mt = (M + 3) >> 2, nt = (N + 3) >> 2;
+        const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
         const int tiles = mt * nt;
-        const int gcn = (ACC ? 1 : G) * nc;
-        const int tid = threadIdx.x;
-        int tile0, tstep, gc0, gcstep;
-        if (tiles >= kThreads) {
-                tile0 = tid; tstep = kThreads; gc0 = 0; gcstep = 1;
-        } else {
-                const int nslot = kThreads / tiles;
-                const int slot = tid / tiles;
-                tile0 = slot < nslot ? tid - slot * tiles : tiles;
-                tstep = tiles;
-                gc0 = slot; gcstep = nslot;
-        }
-        for (int tile = tile0; tile < tiles; tile += tstep) {
+        const int items = (ACC ? 1 : G) * nc * tiles;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int lr = lane >> 2, lc = lane & 3;
+        for (int it = warp; it < items; it += kThreads / 32) {
+                const int tile = it % tiles;
+                const int gc = it / tiles;
                 const int tm = tile % mt, tn = tile / mt;
-                // interleaved micro-tile: rows tm + i*mt, columns tn + j*nt
-                for (int gc = gc0; gc < gcn; gc += gcstep) {
-                        const int c = ACC ? gc : gc % nc;
-                        const int g0 = ACC ? 0 : gc / nc;
-                        const int g1 = ACC ? G : g0 + 1;
-                        double acc[4][4];
-#pragma unroll
-                        for (int i = 0; i < 4; ++i)
-#pragma unroll
-                                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-                        for (int g = g0; g < g1; ++g) {
-                                const double *op = ops + opoff[g];
-                                const double *tin = in + g * in_gs;
-                                const double *Ab = ax == 0 ? op : tin + c * a_cs;
-                                const double *Bb = ax == 0 ? tin : op;
-                                for (int k = 0; k < K; ++k) {
-                                        double a[4], b[4];
-#pragma unroll
-                                        for (int i = 0; i < 4; ++i) {
-                                                const int m = tm + i * mt;
-                                                a[i] = m < M ? Ab[m + k * ak] : 0.0;
-                                        }
-#pragma unroll
-                                        for (int j = 0; j < 4; ++j) {
-                                                const int n = tn + j * nt;
-                                                b[j] = n < N ? Bb[k * bk + n * bn] : 0.0;
-                                        }
-#pragma unroll
-                                        for (int i = 0; i < 4; ++i)
-#pragma unroll
-                                                for (int j = 0; j < 4; ++j)
-                                                        acc[i][j] = fma(a[i], b[j], acc[i][j]);
-                                }
+                const int c = ACC ? gc : gc % nc;
+                const int g0 = ACC ? 0 : gc / nc;
+                const int g1 = ACC ? G : g0 + 1;
+                const int ma = (tm << 3) + lr;          // A row of this lane
+                const int nbb = (tn << 3) + lr;         // B column of this lane
+                const bool mok = ma < M, nok = nbb < N;
+                double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+                for (int g = g0; g < g1; ++g) {
+                        const double *op = ops + opoff[g];
+                        const double *tin = in + g * in_gs;
+                        const double *Ab = (ax == 0 ? op : tin + c * a_cs) + ma;
+                        const double *Bb = (ax == 0 ? tin : op) + nbb * bn;
+                        // k-steps of 4, two accumulator pairs; the loop bounds
+                        // are warp-uniform (mma.sync needs the whole warp) and
+                        // lanes past K load zeros
+                        int k0 = 0;
+                        for (; k0 + 8 <= K; k0 += 8) {
+                                const int k = k0 + lc;
+                                const double a0 = mok ? Ab[k * ak] : 0.0;
+                                const double b0 = nok ? Bb[k * bk] : 0.0;
+                                const double a1 = mok ? Ab[(k + 4) * ak] : 0.0;
+                                const double b1 = nok ? Bb[(k + 4) * bk] : 0.0;
+                                dmma_8x8x4(d0, d1, a0, b0);
+                                dmma_8x8x4(e0, e1, a1, b1);
                         }
+                        for (; k0 < K; k0 += 4) {
+                                const int k = k0 + lc;
+                                const bool kok = k < K;
+                                const double a0 = (mok && kok) ? Ab[k * ak] : 0.0;
+                                const double b0 = (nok && kok) ? Bb[k * bk] : 0.0;
+                                dmma_8x8x4(d0, d1, a0, b0);
+                        }
+                }
+                d0 += e0;
+                d1 += e1;
+                const int mc = (tm << 3) + lr;
+                const int nc0 = (tn << 3) + 2 * lc;
+                if (mc < M) {
                         const double sc = (!ACC && scale) ? scale[g0] : 1.0;
-                        double *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs;
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                                const int m = tm + i * mt;
-                                if (m >= M) continue;
-#pragma unroll
-                                for (int j = 0; j < 4; ++j) {
-                                        const int n = tn + j * nt;
-                                        if (n >= N) continue;
-                                        double *cp = Cb + m + n * cn;
-                                        *cp = ACC ? *cp + acc[i][j] : sc * acc[i][j];
-                                }
+                        double *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs + mc;
+                        if (nc0 < N) {
+                                double *cp = Cb + nc0 * cn;
+                                *cp = ACC ? *cp + d0 : sc * d0;
+                        }
+                        if (nc0 + 1 < N) {
+                                double *cp = Cb + (nc0 + 1) * cn;
+                                *cp = ACC ? *cp + d1 : sc * d1;
                         }
                 }
         }
@@ -170,12 +178,12 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                 const int4 en = edims[nb];
                 const int dn[3] = {en.x, en.y, en.z};
                 // extent and first row of the tile along each axis
-                const int ext[3] = {dn[0], un.bt, un.ct};
-                const int row0[3] = {0, un.b0, un.c0};
+                const int ext[3] = {un.at, un.bt, un.ct};
+                const int row0[3] = {un.a0, un.b0, un.c0};
                 const int st = ext[0] * ext[1] * ext[2];
                 for (int e = tid; e < st; e += kThreads) OUT[e] = 0.0;
                 __syncthreads();
-                for (int p = pair_ptr[nb]; p < pair_ptr[nb + 1]; ++p) {
+                for (int p = un.p0; p < un.p1; ++p) {
                         const HeffPair pr = pairs[p];
                         const int4 eo = edims[pr.old];
                         const int nst = (pr.axes >> 6) & 3;
@@ -239,7 +247,10 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                         const int t = e / ext[0];
                         const int b = t % ext[1];
                         const int c = t / ext[1];
-                        yn[a + (int64_t) dn[0] * ((row0[1] + b) + (int64_t) dn[1] * (row0[2] + c))] = OUT[e];
+                        double *dst = yn + (row0[0] + a) +
+                                      (int64_t) dn[0] * ((row0[1] + b) + (int64_t) dn[1] * (row0[2] + c));
+                        if (un.split) atomicAdd(dst, OUT[e]);
+                        else *dst = OUT[e];
                 }
                 __syncthreads();
         }
@@ -362,8 +373,6 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 if ((int64_t) e[0] * e[1] * e[2] != d->block_off[b + 1] - d->block_off[b])
                         return set_error(T3NS_E_ARG, "block size != product of dims at block " +
                                                           std::to_string(b));
-                if (e[0] > kOutCap)
-                        return set_error(T3NS_E_LIMIT, "leg dimension beyond the output tile");
                 hp.edims[b] = make_int4(e[0], e[1], e[2], 0);
         }
         hp.size = d->block_off[d->nblocks];
@@ -390,14 +399,12 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
         double flops_ref = 0, flops_exec = 0;
         int64_t npairs = 0;
         std::vector<double> unit_work;
+        struct PairTmp { int ob; int t0, t1; int eo[3]; };
+        std::vector<std::vector<PairTmp>> blocks_pairs(d->nblocks);
         for (int nb = 0; nb < d->nblocks; ++nb) {
                 hp.task_ptr[nb] = (int) hp.tasks.size();
-                hp.pair_ptr[nb] = (int) hp.pairs.size();
                 const int dn[3] = {d->dims[3 * nb], d->dims[3 * nb + 1],
                                    d->isdmrg ? 1 : d->dims[3 * nb + 2]};
-                const int4 en4 = hp.edims[nb];
-                const int en[3] = {en4.x, en4.y, en4.z};
-                struct PairTmp { int ob; int t0, t1; int eo[3]; };
                 std::vector<PairTmp> ptmp;
                 for (int p = d->pair_ptr[nb]; p < d->pair_ptr[nb + 1]; ++p) {
                         ++npairs;
@@ -459,22 +466,56 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                 ptmp.push_back({ob, t0, t1, {eo4.x, eo4.y, eo4.z}});
                         }
                 }
+                blocks_pairs[nb] = std::move(ptmp);
+        }
+        hp.task_ptr[d->nblocks] = (int) hp.tasks.size();
+        // a unit should not carry more than a small share of the work, so the
+        // heaviest-first schedule ends evenly across the CTAs
+        const double unit_cap = std::max(flops_ref / (148.0 * 2 * 3), 1e6);
+        for (int nb = 0; nb < d->nblocks; ++nb) {
+                hp.pair_ptr[nb] = (int) hp.pairs.size();
+                auto &ptmp = blocks_pairs[nb];
                 if (ptmp.empty()) continue;
+                const int4 en4 = hp.edims[nb];
+                const int en[3] = {en4.x, en4.y, en4.z};
 
-                // tiling of the output block and a sequence per pair that fits
+                // tiling of the output block and a sequence per pair that fits:
+                // candidates tile one or two memory axes (halving sizes); the
+                // cheapest one whose units stay under the work cap is taken
+                struct Cand { int at, bt, ct; };
+                std::vector<Cand> cand;
                 const int64_t sn = (int64_t) en[0] * en[1] * en[2];
-                std::vector<std::pair<int, int>> cand;   // (bt, ct)
-                if (sn <= kOutCap) cand.push_back({en[1], en[2]});
-                if ((int64_t) en[0] * en[1] <= kOutCap)
-                        for (int ct = (int) std::min<int64_t>(en[2], kOutCap / ((int64_t) en[0] * en[1]));
-                             ct >= 1; ct = ct / 2)
-                                cand.push_back({en[1], ct});
-                for (int bt = std::min(en[1], kOutCap / en[0]); bt >= 1; bt = bt / 2)
-                        cand.push_back({bt, 1});
-                bool placed = false;
-                for (auto [bt, ct] : cand) {
-                        const int mask = (bt < en[1] ? 2 : 0) | (ct < en[2] ? 4 : 0);
-                        const int ext[3] = {en[0], bt, ct};
+                if (sn <= kOutCap) cand.push_back({en[0], en[1], en[2]});
+                for (int ax = 0; ax < 3; ++ax) {
+                        const int64_t rest = sn / std::max(en[ax], 1);
+                        if (rest == 0 || rest > kOutCap) continue;
+                        for (int t = (int) std::min<int64_t>(en[ax], kOutCap / rest); t >= 1; t /= 2) {
+                                if (t == en[ax]) continue;
+                                Cand c{en[0], en[1], en[2]};
+                                (ax == 0 ? c.at : ax == 1 ? c.bt : c.ct) = t;
+                                cand.push_back(c);
+                        }
+                }
+                for (int pair = 0; pair < 3; ++pair) {
+                        // tile axis p1 with t, axis p2 with 1
+                        const int p1 = pair == 2 ? 0 : pair + 1, p2 = pair == 2 ? 1 : (pair == 0 ? 2 : 0);
+                        const int other = 3 - p1 - p2;
+                        if (en[other] > kOutCap || en[p2] <= 1) continue;
+                        for (int t = std::min(en[p1], kOutCap / std::max(en[other], 1)); t >= 1; t /= 2) {
+                                Cand c{en[0], en[1], en[2]};
+                                (p1 == 0 ? c.at : p1 == 1 ? c.bt : c.ct) = t;
+                                (p2 == 0 ? c.at : p2 == 1 ? c.bt : c.ct) = 1;
+                                cand.push_back(c);
+                        }
+                }
+                int best_ci = -1;
+                double best_fl = 0, best_cost = 0;
+                std::vector<int> best_seqs;
+                for (size_t ci = 0; ci < cand.size(); ++ci) {
+                        const Cand &cd = cand[ci];
+                        const int mask = (cd.at < en[0] ? 1 : 0) | (cd.bt < en[1] ? 2 : 0) |
+                                         (cd.ct < en[2] ? 4 : 0);
+                        const int ext[3] = {cd.at, cd.bt, cd.ct};
                         std::vector<int> seqs(ptmp.size());
                         double fl_blk = 0;
                         bool ok = true;
@@ -486,36 +527,79 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                         break;
                                 }
                                 int axes = nops << 6;
-                                for (int s = 0; s < nops; ++s) axes |= seq[s] << (2 * s);
+                                for (int st = 0; st < nops; ++st) axes |= seq[st] << (2 * st);
                                 seqs[q] = axes;
                                 fl_blk += fl * (ptmp[q].t1 - ptmp[q].t0);
                         }
                         if (!ok) continue;
-                        for (size_t q = 0; q < ptmp.size(); ++q)
-                                hp.pairs.push_back({ptmp[q].ob, seqs[q], ptmp[q].t0, ptmp[q].t1});
-                        flops_exec += fl_blk;
-                        const int nbt = (en[1] + bt - 1) / bt, nct = (en[2] + ct - 1) / ct;
-                        for (int ib = 0; ib < nbt; ++ib)
-                                for (int ic = 0; ic < nct; ++ic) {
-                                        HeffUnit u{};
-                                        u.nb = nb;
-                                        u.b0 = ib * bt;
-                                        u.bt = std::min(bt, en[1] - u.b0);
-                                        u.c0 = ic * ct;
-                                        u.ct = std::min(ct, en[2] - u.c0);
-                                        hp.units.push_back(u);
-                                        unit_work.push_back(fl_blk * u.bt * u.ct /
-                                                            ((double) en[1] * en[2]) +
-                                                            1e4 * ptmp.size());
-                                }
-                        placed = true;
-                        break;
+                        // cost: FLOPs plus a fixed charge per (unit, pair) visit
+                        // (staging the old block, group barriers), which keeps
+                        // tiles from shrinking for a marginal FLOP saving
+                        const double nunits = std::ceil((double) en[0] / cd.at) *
+                                              std::ceil((double) en[1] / cd.bt) *
+                                              std::ceil((double) en[2] / cd.ct);
+                        const double cost = fl_blk + kPairVisitCost * nunits * ptmp.size();
+                        if (best_ci < 0 || cost < best_cost) {
+                                best_ci = (int) ci;
+                                best_fl = fl_blk;
+                                best_cost = cost;
+                                best_seqs = seqs;
+                        }
+                }
+                const bool placed = best_ci >= 0;
+                if (placed) {
+                        const Cand cd = cand[best_ci];
+                        const int pbase = (int) hp.pairs.size();
+                        std::vector<double> pfl(ptmp.size());
+                        for (size_t q = 0; q < ptmp.size(); ++q) {
+                                hp.pairs.push_back({ptmp[q].ob, best_seqs[q], ptmp[q].t0, ptmp[q].t1});
+                                int seq[3];
+                                for (int st = 0; st < 3; ++st) seq[st] = (best_seqs[q] >> (2 * st)) & 3;
+                                int64_t s1, s2;
+                                pfl[q] = seq_cost(seq, nops, ptmp[q].eo, en, en, &s1, &s2) *
+                                         (ptmp[q].t1 - ptmp[q].t0);
+                        }
+                        flops_exec += best_fl;
+                        const int nat = (en[0] + cd.at - 1) / cd.at;
+                        const int nbt = (en[1] + cd.bt - 1) / cd.bt, nct = (en[2] + cd.ct - 1) / cd.ct;
+                        for (int ia = 0; ia < nat; ++ia)
+                                for (int ib = 0; ib < nbt; ++ib)
+                                        for (int ic = 0; ic < nct; ++ic) {
+                                                HeffUnit u{};
+                                                u.nb = nb;
+                                                u.a0 = ia * cd.at;
+                                                u.at = std::min(cd.at, en[0] - u.a0);
+                                                u.b0 = ib * cd.bt;
+                                                u.bt = std::min(cd.bt, en[1] - u.b0);
+                                                u.c0 = ic * cd.ct;
+                                                u.ct = std::min(cd.ct, en[2] - u.c0);
+                                                const double frac = ((double) u.at * u.bt * u.ct) / (double) sn;
+                                                // split the tile's pairs into chunks under the cap
+                                                const double tile_work = best_fl * frac;
+                                                const bool split = tile_work > unit_cap && ptmp.size() > 1;
+                                                size_t q = 0;
+                                                while (q < ptmp.size()) {
+                                                        double w = 0;
+                                                        size_t q1 = q;
+                                                        while (q1 < ptmp.size() &&
+                                                               (q1 == q || !split || w + pfl[q1] * frac <= unit_cap)) {
+                                                                w += pfl[q1] * frac;
+                                                                ++q1;
+                                                        }
+                                                        HeffUnit v = u;
+                                                        v.p0 = pbase + (int) q;
+                                                        v.p1 = pbase + (int) q1;
+                                                        v.split = split ? 1 : 0;
+                                                        hp.units.push_back(v);
+                                                        unit_work.push_back(w + 1e4 * (q1 - q));
+                                                        q = q1;
+                                                }
+                                        }
                 }
                 if (!placed)
                         return set_error(T3NS_E_LIMIT, "no tiling of output block " + std::to_string(nb) +
                                                                " fits the shared-memory buffers");
         }
-        hp.task_ptr[d->nblocks] = (int) hp.tasks.size();
         hp.pair_ptr[d->nblocks] = (int) hp.pairs.size();
         if (hp.tasks.size() > (size_t) INT32_MAX)
                 return set_error(T3NS_E_LIMIT, "more than 2^31 tasks");

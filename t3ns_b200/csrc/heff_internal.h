@@ -27,13 +27,18 @@ struct __align__(16) HeffPair {
         int t0, t1;
 };
 
-// One unit of kernel work: the output tile [0,d0) x [b0,b0+bt) x [c0,c0+ct)
-// of new block nb (memory axes), with all of nb's pairs.
+// One unit of kernel work: the output tile [a0,a0+at) x [b0,b0+bt) x
+// [c0,c0+ct) of new block nb (memory axes), over pairs [p0, p1) of nb.
+// When a tile's pairs are split over several units (split != 0) each adds
+// its share into the output with atomics.
 struct __align__(16) HeffUnit {
         int nb;
         int b0, bt;
         int c0, ct;
-        int pad[3];
+        int a0, at;
+        int p0, p1;
+        int split;
+        int pad[2];
 };
 
 struct HostPlan {

@@ -1,10 +1,12 @@
 """Host-side emulation of the matvec work plan (numpy), used to check the
-plan's tiling, contraction sequences and operator row offsets without a GPU.
+plan's tiling, pair splitting, contraction sequences and operator row
+offsets without a GPU.
 
-For selected work units it recomputes the unit's output tile exactly the way
-the kernel organises it -- pair by pair, term by term, contracting the memory
-axes in the pair's sequence, with tiled axes restricted to the tile's rows --
-and returns the tiles for comparison with the reference's matvec output."""
+For selected output blocks it recomputes every work unit of the block the
+way the kernel organises it -- the unit's pairs, term by term, contracting
+the memory axes in the pair's sequence with tiled axes restricted to the
+tile's rows -- adds the units into the block (split units add partial sums)
+and returns the blocks for comparison with the reference's matvec output."""
 import ctypes as C
 import os
 import tempfile
@@ -13,6 +15,8 @@ import numpy as np
 
 from t3ns_b200 import native
 from t3ns_b200.stepfile import read_step
+
+UNIT_FIELDS = 10   # nb, b0, bt, c0, ct, a0, at, p0, p1, split
 
 
 def dump_plan(desc):
@@ -24,51 +28,47 @@ def dump_plan(desc):
         return read_step(p)
 
 
-def op_buffer(s, nops):
-    return np.concatenate([s[f"ops{i}.tel"] for i in range(nops)])
+def units_of(plan):
+    return plan["plan.units"].reshape(-1, UNIT_FIELDS)
 
 
-def emulate_units(s, plan, x, unit_ids):
+def emulate_blocks(s, plan, x, blocks):
     nops = 2 if int(s["isdmrg"][0]) else 3
-    ops = op_buffer(s, nops)
-    units = plan["plan.units"].reshape(-1, 5)
+    ops = np.concatenate([s[f"ops{i}.tel"] for i in range(nops)])
+    units = units_of(plan)
     pairs = plan["plan.pairs"].reshape(-1, 4)
-    pptr = plan["plan.pair_ptr"]
     edims = plan["plan.edims"].reshape(-1, 3)
     offs = plan["plan.op_off"].reshape(-1, 3)
     pref = plan["plan.pref"]
     boff = s["beginblock"].astype(np.int64)
-    out = []
-    for u in unit_ids:
-        nb, b0, bt, c0, ct = (int(v) for v in units[u])
-        dn = edims[nb]
-        ext = [int(dn[0]), bt, ct]
-        row0 = [0, b0, c0]
-        tile = np.zeros(ext[0] * ext[1] * ext[2])
-        for p in range(pptr[nb], pptr[nb + 1]):
-            old, axes, t0, t1 = (int(v) for v in pairs[p])
-            nst = (axes >> 6) & 3
-            seq = [(axes >> (2 * k)) & 3 for k in range(nst)]
-            do = edims[old]
-            psi = x[boff[old]:boff[old + 1]].reshape(do[2], do[1], do[0])   # [c][b][a]
-            for t in range(t0, t1):
-                T = psi
-                for a in seq:
-                    r = ext[a]
-                    op = ops[offs[t, a]: offs[t, a] + dn[a] * do[a]].reshape(do[a], dn[a]).T
-                    op = op[row0[a]:row0[a] + r]                                # (r x do)
-                    ax_np = 2 - a                                              # numpy axis
-                    T = np.moveaxis(np.tensordot(op, T, axes=([1], [ax_np])), 0, ax_np)
-                tile += pref[t] * T.reshape(-1)
-        out.append(tile.reshape(ext[2], ext[1], ext[0]))
+    out = {}
+    for nb in blocks:
+        dn = [int(v) for v in edims[nb]]
+        blk = np.zeros((dn[2], dn[1], dn[0]))
+        for u in np.nonzero(units[:, 0] == nb)[0]:
+            _, b0, bt, c0, ct, a0, at, p0, p1, _split = (int(v) for v in units[u])
+            ext = [at, bt, ct]
+            row0 = [a0, b0, c0]
+            tile = np.zeros((ct, bt, at))
+            for p in range(p0, p1):
+                old, axes, t0, t1 = (int(v) for v in pairs[p])
+                nst = (axes >> 6) & 3
+                seq = [(axes >> (2 * k)) & 3 for k in range(nst)]
+                do = [int(v) for v in edims[old]]
+                psi = x[boff[old]:boff[old + 1]].reshape(do[2], do[1], do[0])   # [c][b][a]
+                for t in range(t0, t1):
+                    T = psi
+                    for a in seq:
+                        op = ops[offs[t, a]: offs[t, a] + dn[a] * do[a]].reshape(do[a], dn[a]).T
+                        op = op[row0[a]:row0[a] + ext[a]]
+                        ax_np = 2 - a
+                        T = np.moveaxis(np.tensordot(op, T, axes=([1], [ax_np])), 0, ax_np)
+                    tile += pref[t] * T
+            blk[c0:c0 + ct, b0:b0 + bt, a0:a0 + at] += tile
+        out[nb] = blk.reshape(-1)
     return out
 
 
-def reference_tile(s, plan, y, u):
-    units = plan["plan.units"].reshape(-1, 5)
-    edims = plan["plan.edims"].reshape(-1, 3)
-    nb, b0, bt, c0, ct = (int(v) for v in units[u])
-    dn = edims[nb]
+def reference_block(s, y, nb):
     boff = s["beginblock"].astype(np.int64)
-    blk = y[boff[nb]:boff[nb + 1]].reshape(dn[2], dn[1], dn[0])
-    return blk[c0:c0 + ct, b0:b0 + bt, :]
+    return y[boff[nb]:boff[nb + 1]]
