@@ -222,23 +222,32 @@ def run_engine(args, rank, world):
     return out
 
 
-def cpu_baseline(path, samples=1, stride=None):
-    """The reference's own matvecT3NS (exec_secondrun) on the host cores, on
-    every `stride`-th output block of the step (a bounded sample)."""
+def cpu_baseline(path, samples=1, stride=None, target_s=15.0):
+    """The reference's own matvecT3NS (exec_secondrun, OpenMP over all host
+    cores, OpenBLAS) on every `stride`-th output block of the step: a bounded
+    sample of about `target_s` seconds, found by a short calibration run on
+    every 64th block."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_matvec_bench")
     if not os.path.exists(exe):
         return None
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    if stride is None:
-        # about 10-30 s of work: the 2.15M-element D=512 step takes ~850 core-s
-        size = os.path.getsize(path)
-        stride = max(1, int(round(850.0 / ncores / 15.0))) if size > 500e6 else 1
     env = dict(os.environ, OMP_NUM_THREADS=str(ncores), OPENBLAS_NUM_THREADS="1")
-    r = subprocess.run([exe, path, str(samples), str(stride)], capture_output=True, text=True,
-                       env=env)
-    if r.returncode != 0:
+
+    def run(n, st):
+        r = subprocess.run([exe, path, str(n), str(st)], capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            return None
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    if stride is None:
+        cal = run(1, 64)
+        if cal is None:
+            return None
+        full_s = cal["seconds_per_matvec"] * 64
+        stride = max(1, int(round(full_s / target_s)))
+    res = run(samples, stride)
+    if res is None:
         return None
-    res = json.loads(r.stdout.strip().splitlines()[-1])
     res["cores"] = ncores
     return res
 

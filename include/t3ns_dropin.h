@@ -1,0 +1,68 @@
+/*
+ * t3ns_dropin.h — the reference entry points exported by libt3ns_dropin.so.
+ *
+ * These are exactly the declarations of the reference's own headers, so the
+ * reference's unchanged sweep driver links against libt3ns_dropin.so in place
+ * of the reference objects Heff.o, davidson.o and wrapper_solvers.o.  The
+ * structs are the reference's (include/Heff.h, include/rOperators.h,
+ * include/siteTensor.h); the library is compiled against those headers
+ * because the driver allocates struct Heffdata itself.  All arithmetic runs
+ * in the engine (t3ns_b200.h) on the GPU.
+ */
+#ifndef T3NS_DROPIN_H
+#define T3NS_DROPIN_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct Heffdata;
+struct rOperators;
+struct siteTensor;
+
+/* Replaces init_Heffdata, reference include/Heff.h:166-167, src/Heff.c:1167-1221:
+ * fills the driver-visible fields of *data (isdmrg, operators, symsecs,
+ * instruction set, nr_qnB) and builds the device plan of the step's matvec. */
+void init_Heffdata(struct Heffdata *data, const struct rOperators *Operators,
+                   const struct siteTensor *siteObject);
+
+/* Replaces matvecT3NS, reference include/Heff.h:177, src/Heff.c:1049-1062:
+ * result = Heff vec on host buffers. */
+void matvecT3NS(const double *vec, double *result, void *vdata);
+
+/* Replaces make_diagonal, reference include/Heff.h:185, src/Heff.c:1268-1312:
+ * returns malloc'd memory that the driver frees. */
+double *make_diagonal(const struct Heffdata *data);
+
+/* Replaces destroy_Heffdata, reference include/Heff.h:192, src/Heff.c:1242-1266. */
+void destroy_Heffdata(struct Heffdata *data);
+
+/* Replaces davidson_diagonal_preconditioner, reference include/davidson.h:36-39,
+ * src/davidson.c:223-257. */
+void davidson_diagonal_preconditioner(const double *result, const double theta, const int size,
+                                      const double *diagonal, double *vec_t);
+
+/* Replaces davidson, reference include/davidson.h:56-60, src/davidson.c:259-328.
+ * With matvec == matvecT3NS the whole solve is device resident; any other
+ * matvec callback is called on host buffers once per iteration. */
+int davidson(double *result, double *energy, int size, int max_vecs, int keep_deflate,
+             double davidson_tol, int max_its, const double *diagonal,
+             void (*matvec)(const double *, double *, void *), void *vdat);
+
+/* Replaces sparse_eigensolve, reference include/wrapper_solvers.h:56-60,
+ * src/wrapper_solvers.c:107-128 ("D" = Davidson; any other name falls back to
+ * Davidson with the reference's message). */
+int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
+                      int keep_deflate, double tol, int max_its, const double *diagonal,
+                      void (*matvec)(const double *, double *, void *), void *vdat,
+                      const char solver[]);
+
+/* Test hook (no counterpart in the reference): writes the compiled schedule
+ * of *data to `path` in the step-file layout without using the GPU. */
+int t3ns_dropin_schedule_write(const struct Heffdata *data, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* T3NS_DROPIN_H */

@@ -1,4 +1,13 @@
-"""Step-file maintenance for the captured workloads (test infrastructure).
+"""Captured step files of the reference sweep (test infrastructure).
+
+``ensure_small()`` runs the reference sweep (oracle/_ref/t3ns_run_ref, built
+by oracle/Makefile) in capture mode for the small cases the GPU parity tests
+use: the Hubbard config (L=10, D=128, all steps of one sweep) and the
+12-orbital synthetic QC Hamiltonian (D=64).  ``ensure_d512()`` captures
+steps 4-6 of the 24-orbital synthetic QC Hamiltonian at D=512 (about ten
+minutes on 8 cores: the initial renormalised operators dominate) and writes
+the structure-only benchmark workloads of steps 5 and 6.  Outputs go to
+oracle/_ref/ (git-ignored).
 
 ``trim(path)`` rewrites a captured step file keeping only the operator
 blocks that the step's schedule references (every other block is marked
@@ -107,7 +116,69 @@ def structure_only(path, out):
     write_step(out, rec)
 
 
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF = os.path.join(HERE, "_ref")
+RUN = os.path.join(REF, "t3ns_run_ref")
+NETS = os.path.join(ROOT, "tests", "golden", "networks")
+
+
+def _fcidump(n):
+    from t3ns_b200.workloads import synthetic_qc_fcidump
+    os.makedirs(os.path.join(REF, "fcidump"), exist_ok=True)
+    return synthetic_qc_fcidump(os.path.join(REF, "fcidump", f"syn{n}.FCIDUMP"), n, n, 0, 72)
+
+
+def _capture(outdir, args, extra, threads):
+    import subprocess
+    os.makedirs(outdir, exist_ok=True)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+    with open(os.path.join(outdir, "run.log"), "w") as log:
+        subprocess.run([RUN, *args, "--init", "c", "--capture", outdir, *extra], check=True,
+                       env=env, stdout=log, stderr=subprocess.STDOUT)
+
+
+def ensure_small(threads=None):
+    threads = threads or os.cpu_count() or 1
+    hub = os.path.join(REF, "captures", "hub10_D128")
+    if not os.path.exists(os.path.join(hub, "step_013.t3c")):
+        _capture(hub, ["--net", os.path.join(NETS, "t3ns_10.netw"), "--inter",
+                       "NN_HUBBARD ( t = 1 U = 4 )", "--symm", "Z2,U1,SU2", "--ts", "0,10,0",
+                       "--regime", "128,128,0,2,1e-5,100,6,1e-8,0"],
+                 ["--capture-limit", "14", "--capture-stop"], threads)
+    qc = os.path.join(REF, "captures", "qc12_D64")
+    if not os.path.exists(os.path.join(qc, "step_017.t3c")):
+        _capture(qc, ["--net", os.path.join(NETS, "t3ns_12.netw"), "--inter", _fcidump(12),
+                      "--symm", "Z2,U1,SU2", "--ts", "0,12,0",
+                      "--regime", "64,64,0,2,1e-5,100,2,1e-8,0"],
+                 ["--capture-limit", "18", "--capture-stop"], threads)
+
+
+def ensure_d512(threads=None):
+    threads = threads or os.cpu_count() or 1
+    d = os.path.join(REF, "captures", "qc24_D512")
+    if not os.path.exists(os.path.join(d, "step_006.t3c")):
+        _capture(d, ["--net", os.path.join(NETS, "t3ns_24.netw"), "--inter", _fcidump(24),
+                     "--symm", "Z2,U1,SU2", "--ts", "0,24,0",
+                     "--regime", "512,512,0,2,1e-5,100,1,1e-8,0"],
+                 ["--capture-min", "60000", "--capture-max", "3000000", "--capture-limit", "3",
+                  "--capture-stop", "--capture-noeig", "--capture-nvec", "2"], threads)
+    wl = os.path.join(REF, "workloads")
+    os.makedirs(wl, exist_ok=True)
+    for step in ("005", "006"):
+        out = os.path.join(wl, f"qc24_D512_step{step}.t3c")
+        src = os.path.join(d, f"step_{step}.t3c")
+        if not os.path.exists(out) and os.path.exists(src):
+            structure_only(src, out)
+
+
 if __name__ == "__main__":
+    if sys.argv[1] == "small":
+        ensure_small()
+        sys.exit(0)
+    if sys.argv[1] == "d512":
+        ensure_d512()
+        sys.exit(0)
     if sys.argv[1] == "structure":
         structure_only(sys.argv[2], sys.argv[3])
         print(sys.argv[3], os.path.getsize(sys.argv[3]) >> 20, "MiB")

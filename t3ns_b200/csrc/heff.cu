@@ -26,8 +26,8 @@
 //     (heaviest first), keeps the unit's output tile in shared memory and
 //     walks its pairs.  A pair's terms share every block dimension and the
 //     contraction order, so G terms at a time go through each stage as one
-//     uniform batched small GEMM on the FP64 tensor pipe (mma.m8n8k4, one
-//     8x8 output tile per warp at a time); the stage before
+//     uniform batched small GEMM on the FP64 tensor pipe (mma.m8n8k4,
+//     register-blocked warp tiles of up to 32x8 / 16x16 / 8x32); the stage before
 //     the last scales by the term prefactor, so the last stage is a plain
 //     reduction over the group inside each warp (single owner per output
 //     element: no atomics).
@@ -63,19 +63,67 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
                      : "d"(a), "d"(b));
 }
 
+// Warp tile of (8*RM) x (8*RN) outputs: RM*RN mma per k-step sharing RM A
+// fragments and RN B fragments, B(k, n) = Bb[k*bk + n*bn]; the next k-step's
+// fragments are loaded before the current step's mma are issued.  Loop
+// bounds are warp-uniform (mma.sync needs the whole warp); lanes outside
+// M, N or K load zeros.
+template <int RM, int RN>
+__device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const double *Ab, int ak,
+                                              const double *Bb, int bk, int bn, int K, int M,
+                                              int N, int m0, int n0, int lr, int lc)
+{
+        bool mok[RM], nok[RN];
+        const double *ap[RM], *bp[RN];
+#pragma unroll
+        for (int i = 0; i < RM; ++i) {
+                const int m = m0 + 8 * i + lr;
+                mok[i] = m < M;
+                ap[i] = Ab + (mok[i] ? m : 0);
+        }
+#pragma unroll
+        for (int j = 0; j < RN; ++j) {
+                const int n = n0 + 8 * j + lr;
+                nok[j] = n < N;
+                bp[j] = Bb + (nok[j] ? n : 0) * bn;
+        }
+        double a[RM], b[RN];
+        auto load = [&](int k0) {
+                const int k = k0 + lc;
+                const bool kok = k < K;
+#pragma unroll
+                for (int i = 0; i < RM; ++i) a[i] = (mok[i] && kok) ? ap[i][k * ak] : 0.0;
+#pragma unroll
+                for (int j = 0; j < RN; ++j) b[j] = (nok[j] && kok) ? bp[j][k * bk] : 0.0;
+        };
+        load(0);
+        for (int k0 = 0; k0 < K; k0 += 4) {
+                double ca[RM], cb[RN];
+#pragma unroll
+                for (int i = 0; i < RM; ++i) ca[i] = a[i];
+#pragma unroll
+                for (int j = 0; j < RN; ++j) cb[j] = b[j];
+                if (k0 + 4 < K) load(k0 + 4);
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) dmma_8x8x4(d[i][j][0], d[i][j][1], ca[i], cb[j]);
+        }
+}
+
 // One contraction stage for G terms.  Term g applies rows [row0, row0+rows)
 // of the operator block at ops + opoff[g] (leading dimension ldop) on axis ax
 // of `in + g * in_gs` (dims w), writing `out + g * out_gs` (scaled by
 // scale[g] when scale != nullptr).  With ACC the G results are summed into
-// `out` instead (which then has no term stride).  Each warp owns 8x8 output
-// tiles and runs their K loop on the FP64 tensor pipe; with ACC the group
-// reduction stays inside the warp's accumulators.
-template <bool ACC>
-__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
-                                              const int64_t *opoff,
-                                              const double *__restrict__ ops, const double *in,
-                                              int in_gs, double *out, int out_gs,
-                                              const double *scale)
+// `out` instead (which then has no term stride).  Each warp owns
+// (8*RM) x (8*RN) output tiles and runs their K loop on the FP64 tensor
+// pipe; with ACC the group reduction stays inside the warp's accumulators.
+template <bool ACC, int RM, int RN>
+__device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, int ldop, int G,
+                                                const int64_t *opoff,
+                                                const double *__restrict__ ops, const double *in,
+                                                int in_gs, double *out, int out_gs,
+                                                const double *scale)
 {
         int M, N, K, nc, ak, bk, bn, cn, a_cs, c_cs;
         // A(m,k) = Ab[m + k*ak], B(k,n) = Bb[k*bk + n*bn], C(m,n) = Cb[m + n*cn]
@@ -90,7 +138,7 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                 M = w[0] * w[1]; N = rows; K = w[2]; nc = 1;
                 ak = M; bk = ldop; bn = 1; cn = M; a_cs = 0; c_cs = 0;
         }
-        const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
+        const int mt = (M + 8 * RM - 1) / (8 * RM), nt = (N + 8 * RN - 1) / (8 * RN);
         const int tiles = mt * nt;
         const int items = (ACC ? 1 : G) * nc * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -102,53 +150,56 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                 const int c = ACC ? gc : gc % nc;
                 const int g0 = ACC ? 0 : gc / nc;
                 const int g1 = ACC ? G : g0 + 1;
-                const int ma = (tm << 3) + lr;          // A row of this lane
-                const int nbb = (tn << 3) + lr;         // B column of this lane
-                const bool mok = ma < M, nok = nbb < N;
-                double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+                const int m0 = tm * 8 * RM, n0 = tn * 8 * RN;
+                double d[RM][RN][2];
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) d[i][j][0] = d[i][j][1] = 0.0;
                 for (int g = g0; g < g1; ++g) {
                         const double *op = ops + opoff[g];
                         const double *tin = in + g * in_gs;
-                        const double *Ab = (ax == 0 ? op : tin + c * a_cs) + ma;
-                        const double *Bb = (ax == 0 ? tin : op) + nbb * bn;
-                        // k-steps of 4, two accumulator pairs; the loop bounds
-                        // are warp-uniform (mma.sync needs the whole warp) and
-                        // lanes past K load zeros
-                        int k0 = 0;
-                        for (; k0 + 8 <= K; k0 += 8) {
-                                const int k = k0 + lc;
-                                const double a0 = mok ? Ab[k * ak] : 0.0;
-                                const double b0 = nok ? Bb[k * bk] : 0.0;
-                                const double a1 = mok ? Ab[(k + 4) * ak] : 0.0;
-                                const double b1 = nok ? Bb[(k + 4) * bk] : 0.0;
-                                dmma_8x8x4(d0, d1, a0, b0);
-                                dmma_8x8x4(e0, e1, a1, b1);
-                        }
-                        for (; k0 < K; k0 += 4) {
-                                const int k = k0 + lc;
-                                const bool kok = k < K;
-                                const double a0 = (mok && kok) ? Ab[k * ak] : 0.0;
-                                const double b0 = (nok && kok) ? Bb[k * bk] : 0.0;
-                                dmma_8x8x4(d0, d1, a0, b0);
-                        }
+                        const double *Ab = ax == 0 ? op : tin + c * a_cs;
+                        const double *Bb = ax == 0 ? tin : op;
+                        warp_tile_mma<RM, RN>(d, Ab, ak, Bb, bk, bn, K, M, N, m0, n0, lr, lc);
                 }
-                d0 += e0;
-                d1 += e1;
-                const int mc = (tm << 3) + lr;
-                const int nc0 = (tn << 3) + 2 * lc;
-                if (mc < M) {
-                        const double sc = (!ACC && scale) ? scale[g0] : 1.0;
-                        double *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs + mc;
-                        if (nc0 < N) {
-                                double *cp = Cb + nc0 * cn;
-                                *cp = ACC ? *cp + d0 : sc * d0;
-                        }
-                        if (nc0 + 1 < N) {
-                                double *cp = Cb + (nc0 + 1) * cn;
-                                *cp = ACC ? *cp + d1 : sc * d1;
+                const double sc = (!ACC && scale) ? scale[g0] : 1.0;
+                double *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs;
+#pragma unroll
+                for (int i = 0; i < RM; ++i) {
+                        const int mc = m0 + 8 * i + lr;
+                        if (mc >= M) continue;
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) {
+                                const int nc0 = n0 + 8 * j + 2 * lc;
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                        if (nc0 + h >= N) continue;
+                                        double *cp = Cb + mc + (nc0 + h) * cn;
+                                        *cp = ACC ? *cp + d[i][j][h] : sc * d[i][j][h];
+                                }
                         }
                 }
         }
+}
+
+// Warp-tile shape per stage: 8x32 when M is small, 32x8 when N is small,
+// else 16x16.
+template <bool ACC>
+__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
+                                              const int64_t *opoff,
+                                              const double *__restrict__ ops, const double *in,
+                                              int in_gs, double *out, int out_gs,
+                                              const double *scale)
+{
+        const int M = ax == 0 ? rows : ax == 1 ? w[0] : w[0] * w[1];
+        const int N = ax == 0 ? w[1] * w[2] : rows;
+        if (M <= 8)
+                grouped_stage_t<ACC, 1, 4>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+        else if (N <= 8)
+                grouped_stage_t<ACC, 4, 1>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+        else
+                grouped_stage_t<ACC, 2, 2>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
 }
 
 __global__ void __launch_bounds__(kThreads, 2)
