@@ -163,6 +163,26 @@ int t3ns_davidson_callback(int64_t size, void (*matvec)(const double *, double *
 int t3ns_precondition_host(int64_t size, const double *result, double theta,
                            const double *diagonal, double *vec_t);
 
+/* Largest vector t3ns_precondition_device_noalloc accepts (elements). */
+#define T3NS_NOALLOC_MAX_SIZE 16777216LL
+
+/* Allocation-free diagonal preconditioner (no counterpart in the reference;
+ * same arithmetic as t3ns_precondition_host).  For callers that cannot
+ * allocate device memory when they need it -- a memory pool or arena that
+ * owns the whole GPU, code that must not trigger the implicit device
+ * synchronisation of cudaMalloc/cudaFree, drivers that forbid allocation
+ * after start-up.  `result`, `diagonal` and `vec_t` are device buffers of
+ * `size` doubles supplied by the caller; vec_t is updated in place on
+ * `stream` (a cudaStream_t).  The reduction scratch is a fixed array inside
+ * the library (about 1 MiB, held by every GPU that loads the library until
+ * exit), so size must not exceed T3NS_NOALLOC_MAX_SIZE (T3NS_E_LIMIT
+ * otherwise).  It calls no allocator.  The first call on a device looks up
+ * the scratch address and should come before any stream capture.  All calls
+ * share the scratch: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int t3ns_precondition_device_noalloc(int64_t size, const double *result, double theta,
+                                     const double *diagonal, double *vec_t, void *stream);
+
 /* Diagnostic: builds the host-side plan of `desc` (no GPU needed) and writes
  * its work units, pair sequences and flattened terms to `path` (step-file
  * record layout), for host-side checks of the tiling and ordering. */

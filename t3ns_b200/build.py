@@ -22,7 +22,7 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu"]
+ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu", "precond_noalloc.cu"]
 
 
 def _run(cmd, cwd=None):

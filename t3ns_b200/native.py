@@ -94,6 +94,9 @@ def load(path: str | None = None):
         lib.t3ns_davidson_device.argtypes = [C.c_void_p, C.c_void_p, _f64p, C.c_int, C.c_int,
                                              C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                                              C.c_void_p]
+    lib.t3ns_precondition_host.argtypes = [C.c_int64, _f64p, C.c_double, _f64p, _f64p]
+    lib.t3ns_precondition_device_noalloc.argtypes = [C.c_int64, C.c_void_p, C.c_double,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p]
     if path is None:
         _lib = lib
     return lib
