@@ -211,7 +211,8 @@ def run_engine(args, rank, world):
                    "parallelism": f"replicas{world}", "l2": "flushed between iterations",
                    "precision": "fp64"},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": traffic_from_profile(path),
                      "peak_source": "measured this run: cuBLAS DGEMM 8192^3 via torch (FP64 "
                                     "peak; MEASURED_PEAKS.json has no FP64 figure)"},
         "e2e": {"value": flops * args.steps * world / t_e2e / 1e12, "unit": UNIT,
@@ -220,6 +221,17 @@ def run_engine(args, rank, world):
         "clocks": clk.summary(),
     }
     return out
+
+
+def traffic_from_profile(workload_path):
+    """DRAM bytes (read + write) of one heff_fp64_kernel launch on this
+    workload, from the ncu capture summarised under profiles/ (None if that
+    workload has not been profiled)."""
+    p = os.path.join(ROOT, "profiles", "heff_fp64_kernel_traffic.json")
+    if not os.path.exists(p):
+        return None
+    rec = json.load(open(p)).get(os.path.basename(workload_path))
+    return None if rec is None else rec["dram_bytes_per_launch"]
 
 
 def cpu_baseline(path, samples=1, stride=None, target_s=15.0):
