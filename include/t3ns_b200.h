@@ -163,6 +163,55 @@ int t3ns_davidson_callback(int64_t size, void (*matvec)(const double *, double *
 int t3ns_precondition_host(int64_t size, const double *result, double theta,
                            const double *diagonal, double *vec_t);
 
+/* Update of a physical renormalised-operator set through its site tensor
+ * (reference update_rOperators_physical, src/rOperators_pUpdate.c:364-387,
+ * pUpdate_block :323-362), flattened.  Every entry couples one updated
+ * operator block (a "unit" groups the entries with the same updated block)
+ * to one original block through the site-tensor block T and its adjoint
+ * block Ta:
+ *   left  (is_left):  U_i += pref * Ta^T O_i T   (O_i: M0 x M1, T: M1 x N1,
+ *                                                 Ta: M0 x N0, U_i: N0 x N1)
+ *   right:            U_i += pref * Ta O_i T^T   (T: N1 x M1, Ta: N0 x M0)
+ * for every operator i of the entry's MPO sector whose two blocks are
+ * present (op pair list).  Offsets index the site-tensor elements, the
+ * concatenation of the original operators' elements, and the concatenation
+ * of the updated operators' elements. */
+typedef struct {
+        int is_left;
+        int nunits;
+        const int *unit_ptr;        /* [nunits + 1] CSR into entries          */
+        int nentries;
+        const int *dims;            /* [nentries * 4]: M0, M1, N0, N1         */
+        const int64_t *t_off;       /* [nentries] T block                     */
+        const int64_t *ta_off;      /* [nentries] adjoint block               */
+        const double *pref;         /* [nentries] symmetry prefactor          */
+        const int *op_ptr;          /* [nentries + 1] CSR into op pairs       */
+        const int64_t *old_off;     /* [npairs] original operator block       */
+        const int64_t *new_off;     /* [npairs] updated operator block        */
+        int64_t t_elems, old_elems, new_elems;
+} t3ns_pupdate_desc;
+
+/* Runs a physical update on host buffers: new_tel (new_elems doubles) is
+ * overwritten with the updated operators' elements. */
+int t3ns_pupdate_host(const t3ns_pupdate_desc *d, const double *t_tel, const double *old_tel,
+                      double *new_tel);
+
+/* Scaled block copies: dst[dst_off[e] + j] = scale[e] * src[src_off[e] + j]
+ * for j < len[e]; every other element of dst is zero.  This is the
+ * arithmetic of appending a site operator to a renormalised-operator set
+ * (reference rOperators_append_phys / pAppend_block,
+ * src/rOperators_pUpdate.c:537-640, 665-673). */
+typedef struct {
+        int nentries;
+        const int64_t *dst_off;
+        const int64_t *src_off;
+        const int *len;
+        const double *scale;
+        int64_t src_elems, dst_elems;
+} t3ns_scalecopy_desc;
+
+int t3ns_scalecopy_host(const t3ns_scalecopy_desc *d, const double *src, double *dst);
+
 /* Largest vector t3ns_precondition_device_noalloc accepts (elements). */
 #define T3NS_NOALLOC_MAX_SIZE 16777216LL
 

@@ -129,12 +129,13 @@ def _fcidump(n):
     return synthetic_qc_fcidump(os.path.join(REF, "fcidump", f"syn{n}.FCIDUMP"), n, n, 0, 72)
 
 
-def _capture(outdir, args, extra, threads):
+def _capture(outdir, args, extra, threads, steps=True):
     import subprocess
     os.makedirs(outdir, exist_ok=True)
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+    cap = ["--capture", outdir] if steps else []
     with open(os.path.join(outdir, "run.log"), "w") as log:
-        subprocess.run([RUN, *args, "--init", "c", "--capture", outdir, *extra], check=True,
+        subprocess.run([RUN, *args, "--init", "c", *cap, *extra], check=True,
                        env=env, stdout=log, stderr=subprocess.STDOUT)
 
 
@@ -152,6 +153,25 @@ def ensure_small(threads=None):
                       "--symm", "Z2,U1,SU2", "--ts", "0,12,0",
                       "--regime", "64,64,0,2,1e-5,100,2,1e-8,0"],
                  ["--capture-limit", "18", "--capture-stop"], threads)
+
+
+def ensure_updates(threads=None):
+    """Physical-update captures (inputs, the drop-in's compiled schedule,
+    the reference output) over one sweep of the Hubbard and QC12 cases."""
+    threads = threads or os.cpu_count() or 1
+    lib = os.path.join(ROOT, "t3ns_b200", "_lib", "libt3ns_dropin.so")
+    for name, args in [
+        ("pupdate_hub10", ["--net", os.path.join(NETS, "t3ns_10.netw"), "--inter",
+                           "NN_HUBBARD ( t = 1 U = 4 )", "--symm", "Z2,U1,SU2", "--ts", "0,10,0",
+                           "--regime", "128,128,0,2,1e-5,100,1,1e-8,0"]),
+        ("pupdate_qc12", ["--net", os.path.join(NETS, "t3ns_12.netw"), "--inter", _fcidump(12),
+                          "--symm", "Z2,U1,SU2", "--ts", "0,12,0",
+                          "--regime", "64,64,0,2,1e-5,100,1,1e-8,0"])]:
+        d = os.path.join(REF, "captures", name)
+        if os.path.exists(os.path.join(d, "run.log")):
+            continue
+        _capture(d, args, ["--capture-pupdate", d, "--capture-pupdate-limit", "60",
+                           "--schedule-lib", lib], threads, steps=False)
 
 
 def ensure_d512(threads=None):
@@ -175,6 +195,9 @@ def ensure_d512(threads=None):
 if __name__ == "__main__":
     if sys.argv[1] == "small":
         ensure_small()
+        sys.exit(0)
+    if sys.argv[1] == "updates":
+        ensure_updates()
         sys.exit(0)
     if sys.argv[1] == "d512":
         ensure_d512()

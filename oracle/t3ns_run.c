@@ -74,6 +74,9 @@ static int opt_capture_stop;             /* exit after the last capture */
 static int opt_capture_nvec = 2;         /* seeded matvec pairs         */
 static int opt_capture_noeig;            /* skip Davidson in capture    */
 static const char *opt_schedule_lib;     /* drop-in whose schedule to dump */
+static const char *opt_capture_pupdate;  /* dir for physical-update captures */
+static int opt_pupdate_limit = 4;
+static int opt_pupdate_count;
 static int opt_step_counter;
 static int opt_captured;
 
@@ -332,6 +335,63 @@ static int capture_step(struct Heffdata *hd, double *guess, int size,
 }
 
 #ifndef T3NS_RUN_DROPIN
+static void dump_siteTensor(const char *pre, const struct siteTensor *t)
+{
+        char nm[64];
+        snprintf(nm, sizeof nm, "%s.nrsites", pre);
+        cap_int(nm, t->nrsites);
+        snprintf(nm, sizeof nm, "%s.sites", pre);
+        cap_i32(nm, t->nrsites, t->sites);
+        snprintf(nm, sizeof nm, "%s.nrblocks", pre);
+        cap_int(nm, t->nrblocks);
+        snprintf(nm, sizeof nm, "%s.qnumbers", pre);
+        cap_i64(nm, (int64_t) t->nrblocks * t->nrsites, (const int64_t *) t->qnumbers);
+        snprintf(nm, sizeof nm, "%s.beginblock", pre);
+        cap_i32(nm, t->nrblocks + 1, t->blocks.beginblock);
+        snprintf(nm, sizeof nm, "%s.tel", pre);
+        cap_f64(nm, t->blocks.beginblock[t->nrblocks], t->blocks.tel);
+}
+
+/* Captures the reference's physical update: its inputs, the product's
+ * compiled schedule for them (loaded privately from --schedule-lib), and the
+ * reference's output.  Interposes the reference's update_rOperators_physical
+ * (src/rOperators_pUpdate.c:364-387). */
+typedef void (*pupd_fn)(struct rOperators *, const struct siteTensor *, const struct symsecs *);
+void update_rOperators_physical(struct rOperators *rops, const struct siteTensor *tens,
+                                const struct symsecs *internalss)
+{
+        static pupd_fn real;
+        if (!real) real = (pupd_fn) dlsym(RTLD_NEXT, "update_rOperators_physical");
+        const int want = opt_capture_pupdate && opt_pupdate_count < opt_pupdate_limit;
+        char path[4096];
+        if (want) {
+                snprintf(path, sizeof path, "%s/pupdate_%03d.t3c", opt_capture_pupdate, opt_pupdate_count);
+                cap_fp = fopen(path, "wb");
+                if (!cap_fp) { perror(path); exit(EXIT_FAILURE); }
+                fwrite("T3NSCAP1", 1, 8, cap_fp);
+                dump_rops(0, rops);
+                dump_siteTensor("T", tens);
+                if (opt_schedule_lib) {
+                        void *h = dlopen(opt_schedule_lib, RTLD_NOW | RTLD_LOCAL);
+                        int (*wr)(const struct rOperators *, const struct siteTensor *,
+                                  const struct symsecs *, const char *) =
+                                h ? dlsym(h, "t3ns_dropin_pupdate_write") : NULL;
+                        if (!wr) { fprintf(stderr, "no t3ns_dropin_pupdate_write\n"); exit(EXIT_FAILURE); }
+                        char sp[4096];
+                        snprintf(sp, sizeof sp, "%s/pupdate_%03d.sched", opt_capture_pupdate,
+                                 opt_pupdate_count);
+                        if (wr(rops, tens, internalss, sp) != 0) exit(EXIT_FAILURE);
+                }
+        }
+        real(rops, tens, internalss);
+        if (want) {
+                dump_rops(1, rops);
+                fclose(cap_fp);
+                cap_fp = NULL;
+                ++opt_pupdate_count;
+        }
+}
+
 int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
                       int keep_deflate, double tol, int max_its,
                       const double *diagonal,
@@ -407,6 +467,8 @@ int main(int argc, char **argv)
                 else if (!strcmp(a, "--capture-stop")) { opt_capture_stop = 1; }
                 else if (!strcmp(a, "--capture-noeig")) { opt_capture_noeig = 1; }
                 else if (!strcmp(a, "--schedule-lib") && v) { opt_schedule_lib = v; ++i; }
+                else if (!strcmp(a, "--capture-pupdate") && v) { opt_capture_pupdate = v; ++i; }
+                else if (!strcmp(a, "--capture-pupdate-limit") && v) { opt_pupdate_limit = atoi(v); ++i; }
                 else if (!strcmp(a, "--regime") && v) {
                         struct regime *r = &regs[nreg++];
                         memset(r, 0, sizeof *r);

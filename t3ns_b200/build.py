@@ -22,7 +22,7 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu", "precond_noalloc.cu"]
+ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu", "precond_noalloc.cu", "rops_update.cu"]
 
 
 def _run(cmd, cwd=None):
@@ -57,6 +57,7 @@ def build_engine(force: bool = False) -> str:
 
 REFERENCE_INCLUDE = os.environ.get("T3NS_REFERENCE_INCLUDE", "/root/reference/include")
 SHIM_INCLUDE = os.path.join(ROOT, "oracle", "shim")
+DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c"]
 
 
 def build_dropin(force: bool = False):
@@ -67,11 +68,11 @@ def build_dropin(force: bool = False):
         return None
     engine = build_engine()
     out = os.path.join(LIBDIR, "libt3ns_dropin.so")
-    src = os.path.join(CSRC, "dropin", "heff_dropin.c")
-    if force or _stale(out, [src, engine, os.path.join(INCLUDE, "t3ns_b200.h")]):
+    srcs = [os.path.join(CSRC, "dropin", f) for f in DROPIN_SOURCES]
+    if force or _stale(out, srcs + [engine, os.path.join(INCLUDE, "t3ns_b200.h")]):
         _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu11", "-w", "-DMAX_SYMMETRIES=5",
               "-DNDEBUG", "-I", REFERENCE_INCLUDE, "-I", SHIM_INCLUDE, "-I", INCLUDE,
-              "-o", out, src, "-L", LIBDIR, "-l:libt3ns_b200.so", "-Wl,-rpath,$ORIGIN",
+              "-o", out, *srcs, "-L", LIBDIR, "-l:libt3ns_b200.so", "-Wl,-rpath,$ORIGIN",
               "-lpthread"])
     return out
 

@@ -522,7 +522,7 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
         hp.task_ptr[d->nblocks] = (int) hp.tasks.size();
         // a unit should not carry more than a small share of the work, so the
         // heaviest-first schedule ends evenly across the CTAs
-        const double unit_cap = std::max(flops_ref / (148.0 * 2 * 3), 1e6);
+        const double unit_cap = std::max(flops_ref / (148.0 * 2 * 8), 1e6);
         for (int nb = 0; nb < d->nblocks; ++nb) {
                 hp.pair_ptr[nb] = (int) hp.pairs.size();
                 auto &ptmp = blocks_pairs[nb];
@@ -627,14 +627,16 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                                 const double frac = ((double) u.at * u.bt * u.ct) / (double) sn;
                                                 // split the tile's pairs into chunks under the cap
                                                 const double tile_work = best_fl * frac;
-                                                const bool split = tile_work > unit_cap && ptmp.size() > 1;
+                                                const bool split = tile_work + kPairVisitCost * ptmp.size() > unit_cap &&
+                                                                   ptmp.size() > 1;
                                                 size_t q = 0;
                                                 while (q < ptmp.size()) {
                                                         double w = 0;
                                                         size_t q1 = q;
                                                         while (q1 < ptmp.size() &&
-                                                               (q1 == q || !split || w + pfl[q1] * frac <= unit_cap)) {
-                                                                w += pfl[q1] * frac;
+                                                               (q1 == q || !split ||
+                                                                w + pfl[q1] * frac + kPairVisitCost <= unit_cap)) {
+                                                                w += pfl[q1] * frac + kPairVisitCost;
                                                                 ++q1;
                                                         }
                                                         HeffUnit v = u;

@@ -20,7 +20,17 @@ def golden_steps():
 def captured_steps(max_bytes=400 << 20):
     """Step files captured at build time (oracle/_ref/captures), small ones."""
     out = []
-    for p in sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "captures", "*", "*.t3c"))):
+    for p in sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "captures", "*", "step_*.t3c"))):
         if os.path.getsize(p) <= max_bytes:
+            out.append(p)
+    return out
+
+
+def pupdate_captures():
+    """Physical-update captures with their compiled schedules."""
+    out = []
+    for p in sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "captures", "pupdate_*",
+                                           "pupdate_*.t3c"))):
+        if os.path.exists(p.replace(".t3c", ".sched")):
             out.append(p)
     return out
