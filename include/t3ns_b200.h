@@ -212,6 +212,34 @@ typedef struct {
 
 int t3ns_scalecopy_host(const t3ns_scalecopy_desc *d, const double *src, double *dst);
 
+/* Update through a branching tensor (reference update_rOperators_branching,
+ * src/rOperators_bUpdate.c:229-248, update_selected_blocks :1043-1072),
+ * flattened.  An entry couples one block of each input operator set
+ * (O1 on memory axis ax[0] of the site tensor, O2 on axis ax[1]), the
+ * site-tensor block T (ket indices, dims kd[3]) and the block Ta at the bra
+ * indices (dims bd[3]); for each op triple of the entry
+ *   New(b_g, k_g) += pref * sum Ta(b) O1(b_a, k_a) O2(b_b, k_b) T(k)
+ * summing over the bra and ket indices of axes ax[0], ax[1] (g = ax[2]).
+ * Operator blocks are (bra x ket) column-major.  Units group the entries of
+ * one new block and run concurrently, so the new blocks a unit writes must
+ * not be written by any other unit; new_tel is overwritten (zero + sums). */
+typedef struct {
+        int ax[3];
+        int nunits;
+        const int *unit_ptr;        /* [nunits + 1] CSR into entries           */
+        int nentries;
+        const int *dims;            /* [nentries * 6]: kd[0..2], bd[0..2]      */
+        const int64_t *t_off;       /* [nentries] T block (ket indices)        */
+        const int64_t *ta_off;      /* [nentries] T block at the bra indices   */
+        const double *pref;         /* [nentries]                              */
+        const int *op_ptr;          /* [nentries + 1] CSR into op triples      */
+        const int64_t *o1_off, *o2_off, *new_off;   /* [ntriples]              */
+        int64_t t_elems, o1_elems, o2_elems, new_elems;
+} t3ns_bupdate_desc;
+
+int t3ns_bupdate_host(const t3ns_bupdate_desc *d, const double *t_tel, const double *o1_tel,
+                      const double *o2_tel, double *new_tel);
+
 /* Largest vector t3ns_precondition_device_noalloc accepts (elements). */
 #define T3NS_NOALLOC_MAX_SIZE 16777216LL
 

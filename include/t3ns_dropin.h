@@ -3,7 +3,8 @@
  *
  * These are exactly the declarations of the reference's own headers, so the
  * reference's unchanged sweep driver links against libt3ns_dropin.so in place
- * of the reference objects Heff.o, davidson.o and wrapper_solvers.o.  The
+ * of the reference objects Heff.o, davidson.o, wrapper_solvers.o,
+ * rOperators_pUpdate.o and rOperators_bUpdate.o.  The
  * structs are the reference's (include/Heff.h, include/rOperators.h,
  * include/siteTensor.h); the library is compiled against those headers
  * because the driver allocates struct Heffdata itself.  All arithmetic runs
@@ -19,6 +20,7 @@ extern "C" {
 struct Heffdata;
 struct rOperators;
 struct siteTensor;
+struct symsecs;
 
 /* Replaces init_Heffdata, reference include/Heff.h:166-167, src/Heff.c:1167-1221:
  * fills the driver-visible fields of *data (isdmrg, operators, symsecs,
@@ -57,9 +59,33 @@ int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
                       void (*matvec)(const double *, double *, void *), void *vdat,
                       const char solver[]);
 
+/* Replaces update_rOperators_physical, reference include/rOperators.h:276-278,
+ * src/rOperators_pUpdate.c:364-387: *rops is destroyed and replaced by the
+ * set renormalised through the physical site tensor tens. */
+void update_rOperators_physical(struct rOperators *rops, const struct siteTensor *tens,
+                                const struct symsecs *internalss);
+
+/* Replaces rOperators_append_phys, reference include/rOperators.h:265-266,
+ * src/rOperators_pUpdate.c:665-673: *newrops receives oldrops with the site
+ * operators of the next physical site appended. */
+void rOperators_append_phys(struct rOperators *newrops, const struct rOperators *oldrops);
+
+/* Replaces update_rOperators_branching, reference include/rOperators.h:289-291,
+ * src/rOperators_bUpdate.c:229-248: *newops receives the set on the free bond
+ * of the branching tensor tens, built from Operator[0] and Operator[1]. */
+void update_rOperators_branching(struct rOperators *newops, const struct rOperators *Operator,
+                                 const struct siteTensor *tens);
+
 /* Test hook (no counterpart in the reference): writes the compiled schedule
  * of *data to `path` in the step-file layout without using the GPU. */
 int t3ns_dropin_schedule_write(const struct Heffdata *data, const char *path);
+
+/* Test hooks (no counterpart in the reference): the compiled schedules of a
+ * physical and of a branching update, written to `path` without the GPU. */
+int t3ns_dropin_pupdate_write(const struct rOperators *rops, const struct siteTensor *tens,
+                              const struct symsecs *internalss, const char *path);
+int t3ns_dropin_bupdate_write(const struct rOperators *Operator, const struct siteTensor *tens,
+                              const char *path);
 
 #ifdef __cplusplus
 }

@@ -392,6 +392,47 @@ void update_rOperators_physical(struct rOperators *rops, const struct siteTensor
         }
 }
 
+/* Captures the reference's branching update the same way: both input sets
+ * (ops0, ops1), the branching tensor, the product's compiled schedule and the
+ * reference's output (ops2).  Interposes update_rOperators_branching
+ * (src/rOperators_bUpdate.c:229-248). */
+typedef void (*bupd_fn)(struct rOperators *, const struct rOperators *, const struct siteTensor *);
+static int opt_bupdate_count;
+void update_rOperators_branching(struct rOperators *newops, const struct rOperators *Operator,
+                                 const struct siteTensor *tens)
+{
+        static bupd_fn real;
+        if (!real) real = (bupd_fn) dlsym(RTLD_NEXT, "update_rOperators_branching");
+        const int want = opt_capture_pupdate && opt_bupdate_count < opt_pupdate_limit;
+        if (want) {
+                char path[4096];
+                snprintf(path, sizeof path, "%s/bupdate_%03d.t3c", opt_capture_pupdate, opt_bupdate_count);
+                cap_fp = fopen(path, "wb");
+                if (!cap_fp) { perror(path); exit(EXIT_FAILURE); }
+                fwrite("T3NSCAP1", 1, 8, cap_fp);
+                dump_rops(0, &Operator[0]);
+                dump_rops(1, &Operator[1]);
+                dump_siteTensor("T", tens);
+                if (opt_schedule_lib) {
+                        void *h = dlopen(opt_schedule_lib, RTLD_NOW | RTLD_LOCAL);
+                        int (*wr)(const struct rOperators *, const struct siteTensor *, const char *) =
+                                h ? dlsym(h, "t3ns_dropin_bupdate_write") : NULL;
+                        if (!wr) { fprintf(stderr, "no t3ns_dropin_bupdate_write\n"); exit(EXIT_FAILURE); }
+                        char sp[4096];
+                        snprintf(sp, sizeof sp, "%s/bupdate_%03d.sched", opt_capture_pupdate,
+                                 opt_bupdate_count);
+                        if (wr(Operator, tens, sp) != 0) exit(EXIT_FAILURE);
+                }
+        }
+        real(newops, Operator, tens);
+        if (want) {
+                dump_rops(2, newops);
+                fclose(cap_fp);
+                cap_fp = NULL;
+                ++opt_bupdate_count;
+        }
+}
+
 int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
                       int keep_deflate, double tol, int max_its,
                       const double *diagonal,

@@ -57,7 +57,7 @@ def build_engine(force: bool = False) -> str:
 
 REFERENCE_INCLUDE = os.environ.get("T3NS_REFERENCE_INCLUDE", "/root/reference/include")
 SHIM_INCLUDE = os.path.join(ROOT, "oracle", "shim")
-DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c"]
+DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c", "bupdate_dropin.c"]
 
 
 def build_dropin(force: bool = False):

@@ -1,6 +1,6 @@
 /* Reference-ABI drop-in for the physical renormalised-operator update.
  *
- * Exports update_rOperators_physical (reference include/rOperators.h:277-279,
+ * Exports update_rOperators_physical (reference include/rOperators.h:276-278,
  * src/rOperators_pUpdate.c:364-387) with the reference's signature and
  * ownership rules: the input set is destroyed and replaced by the updated
  * one, whose arrays are host malloc memory the driver later frees.  The
@@ -35,22 +35,11 @@
 #include "symsecs.h"
 
 #include "t3ns_b200.h"
-
-struct pu_vec { void *a; int64_t n, cap; size_t el; };
-
-static void pu_push(struct pu_vec *v, const void *x)
-{
-        if (v->n == v->cap) {
-                v->cap = v->cap ? 2 * v->cap : 256;
-                v->a = realloc(v->a, v->el * (size_t) v->cap);
-                if (!v->a) { fprintf(stderr, "t3ns drop-in: out of memory\n"); exit(EXIT_FAILURE); }
-        }
-        memcpy((char *) v->a + v->el * (size_t) v->n++, x, v->el);
-}
+#include "dropin_util.h"
 
 struct pu_sched {
         struct rOperators ur;        /* updated operators (structure + calloc'd tel) */
-        struct pu_vec unit_ptr, dims, t_off, ta_off, pref, op_ptr, old_off, new_off;
+        struct dv_vec unit_ptr, dims, t_off, ta_off, pref, op_ptr, old_off, new_off;
         int64_t *old_base, *new_base;
         int64_t old_elems, new_elems;
 };
@@ -173,23 +162,23 @@ static void pu_compile(const struct rOperators *rops, const struct siteTensor *T
                                 if (!get_size_block(ob_, osb2) || !get_size_block(nb_, usb2)) continue;
                                 const int64_t oo = S->old_base[i] + ob_->beginblock[osb2];
                                 const int64_t no = S->new_base[i] + nb_->beginblock[usb2];
-                                pu_push(&S->old_off, &oo);
-                                pu_push(&S->new_off, &no);
+                                dv_push(&S->old_off, &oo);
+                                dv_push(&S->new_off, &no);
                         }
                         if ((int) S->old_off.n == first_pair) continue;
                         const int dm[4] = {M0, M1, N0, N1};
-                        for (int k = 0; k < 4; ++k) pu_push(&S->dims, &dm[k]);
+                        for (int k = 0; k < 4; ++k) dv_push(&S->dims, &dm[k]);
                         const int64_t to = T->blocks.beginblock[Tsb], tao = T->blocks.beginblock[Thsb];
-                        pu_push(&S->t_off, &to);
-                        pu_push(&S->ta_off, &tao);
-                        pu_push(&S->pref, &pref);
-                        pu_push(&S->op_ptr, &first_pair);
+                        dv_push(&S->t_off, &to);
+                        dv_push(&S->ta_off, &tao);
+                        dv_push(&S->pref, &pref);
+                        dv_push(&S->op_ptr, &first_pair);
                 }
-                if ((int) S->pref.n > entries_before) pu_push(&S->unit_ptr, &entries_before);
+                if ((int) S->pref.n > entries_before) dv_push(&S->unit_ptr, &entries_before);
         }
         const int ne = (int) S->pref.n, np = (int) S->old_off.n;
-        pu_push(&S->unit_ptr, &ne);
-        pu_push(&S->op_ptr, &np);
+        dv_push(&S->unit_ptr, &ne);
+        dv_push(&S->op_ptr, &np);
 }
 
 static void pu_free(struct pu_sched *S)
@@ -228,21 +217,14 @@ void update_rOperators_physical(struct rOperators *rops, const struct siteTensor
         t3ns_pupdate_desc d;
         pu_desc(&S, rops, tens, &d);
 
-        double *old_tel = safe_malloc(S.old_elems + 1, double);
+        double *old_tel = dropin_gather(rops, S.old_base);
         double *new_tel = safe_malloc(S.new_elems + 1, double);
-        for (int i = 0; i < rops->nrops; ++i)
-                if (S.old_base[i + 1] > S.old_base[i])
-                        memcpy(old_tel + S.old_base[i], rops->operators[i].tel,
-                               sizeof(double) * (size_t) (S.old_base[i + 1] - S.old_base[i]));
         if (t3ns_pupdate_host(&d, tens->blocks.tel, old_tel, new_tel) != T3NS_OK) {
                 fprintf(stderr, "t3ns drop-in: update_rOperators_physical: %s\n", t3ns_last_error());
                 exit(EXIT_FAILURE);
         }
         struct rOperators *ur = &S.ur;
-        for (int i = 0; i < ur->nrops; ++i)
-                if (S.new_base[i + 1] > S.new_base[i])
-                        memcpy(ur->operators[i].tel, new_tel + S.new_base[i],
-                               sizeof(double) * (size_t) (S.new_base[i + 1] - S.new_base[i]));
+        dropin_scatter(ur, S.new_base, new_tel);
         safe_free(old_tel);
         safe_free(new_tel);
         /* the reference's cleanup_update (:181-190): the original set is
@@ -264,49 +246,27 @@ int t3ns_dropin_pupdate_write(const struct rOperators *rops, const struct siteTe
         FILE *f = fopen(path, "wb");
         if (!f) return -1;
         fwrite("T3NSCAP1", 1, 8, f);
-        struct { const char *n; int t; int64_t c; const void *a; } recs[] = {
-                {"pu.unit_ptr", 1, S.unit_ptr.n, S.unit_ptr.a},
-                {"pu.dims", 1, S.dims.n, S.dims.a},
-                {"pu.t_off", 2, S.t_off.n, S.t_off.a},
-                {"pu.ta_off", 2, S.ta_off.n, S.ta_off.a},
-                {"pu.pref", 3, S.pref.n, S.pref.a},
-                {"pu.op_ptr", 1, S.op_ptr.n, S.op_ptr.a},
-                {"pu.old_off", 2, S.old_off.n, S.old_off.a},
-                {"pu.new_off", 2, S.new_off.n, S.new_off.a},
-                {"pu.new_base", 2, (int64_t) rops->nrops + 1, S.new_base},
-        };
-        for (size_t r = 0; r < sizeof recs / sizeof recs[0]; ++r) {
-                char nm[48] = {0};
-                strncpy(nm, recs[r].n, sizeof nm - 1);
-                int32_t hdr[2] = {recs[r].t, 0};
-                fwrite(nm, 1, sizeof nm, f);
-                fwrite(hdr, sizeof hdr, 1, f);
-                fwrite(&recs[r].c, sizeof recs[r].c, 1, f);
-                if (recs[r].c) fwrite(recs[r].a, recs[r].t == 1 ? 4 : 8, (size_t) recs[r].c, f);
-        }
+        dropin_rec(f, "pu.unit_ptr", 1, S.unit_ptr.n, S.unit_ptr.a);
+        dropin_rec(f, "pu.dims", 1, S.dims.n, S.dims.a);
+        dropin_rec(f, "pu.t_off", 2, S.t_off.n, S.t_off.a);
+        dropin_rec(f, "pu.ta_off", 2, S.ta_off.n, S.ta_off.a);
+        dropin_rec(f, "pu.pref", 3, S.pref.n, S.pref.a);
+        dropin_rec(f, "pu.op_ptr", 1, S.op_ptr.n, S.op_ptr.a);
+        dropin_rec(f, "pu.old_off", 2, S.old_off.n, S.old_off.a);
+        dropin_rec(f, "pu.new_off", 2, S.new_off.n, S.new_off.a);
+        dropin_rec(f, "pu.new_base", 2, (int64_t) rops->nrops + 1, S.new_base);
         /* the updated set's block layout before zero-block removal */
         {
-                struct pu_vec bb = {0, 0, 0, sizeof(int)};
+                struct dv_vec bb = {0, 0, 0, sizeof(int)};
                 for (int i = 0; i < S.ur.nrops; ++i) {
                         const int nbn = nblocks_in_operator(&S.ur, i);
-                        for (int b = 0; b <= nbn; ++b) pu_push(&bb, &S.ur.operators[i].beginblock[b]);
+                        for (int b = 0; b <= nbn; ++b) dv_push(&bb, &S.ur.operators[i].beginblock[b]);
                 }
-                char nm2[48] = "pu.new_beginblock";
-                int32_t h2[2] = {1, 0};
-                fwrite(nm2, 1, sizeof nm2, f);
-                fwrite(h2, sizeof h2, 1, f);
-                fwrite(&bb.n, sizeof bb.n, 1, f);
-                if (bb.n) fwrite(bb.a, 4, (size_t) bb.n, f);
+                dropin_rec(f, "pu.new_beginblock", 1, bb.n, bb.a);
                 free(bb.a);
         }
         const int il = rops->is_left == 1;
-        char nm[48] = "pu.is_left";
-        int32_t hdr[2] = {1, 0};
-        int64_t one = 1;
-        fwrite(nm, 1, sizeof nm, f);
-        fwrite(hdr, sizeof hdr, 1, f);
-        fwrite(&one, sizeof one, 1, f);
-        fwrite(&il, sizeof il, 1, f);
+        dropin_rec(f, "pu.is_left", 1, 1, &il);
         fclose(f);
         destroy_rOperators(&S.ur);
         pu_free(&S);
@@ -315,7 +275,7 @@ int t3ns_dropin_pupdate_write(const struct rOperators *rops, const struct siteTe
 
 /* ------------------------------------------------------------------ */
 /* Appending a site operator: rOperators_append_phys (reference
- * include/rOperators.h:273-274, src/rOperators_pUpdate.c:665-673).
+ * include/rOperators.h:265-266, src/rOperators_pUpdate.c:665-673).
  *
  * The unique appended operators (init_unique_rOperators, :393-423) are built
  * from the instruction set of fetch_pUpdate; each of their blocks is the
@@ -328,29 +288,6 @@ int t3ns_dropin_pupdate_write(const struct rOperators *rops, const struct siteTe
 
 struct pa_ops { int po, so, hss[3]; };
 
-static void pa_init_unique(struct rOperators *ur, int bond, int il,
-                           const struct instructionset *set)
-{
-        int **tmpbb;
-        init_rOperators(ur, &tmpbb, bond, il, true);
-        int cinstr = -1;
-        ur->nrops = 0;
-        while (get_next_unique_instr(&cinstr, set)) ++ur->nrops;
-        ur->hss_of_ops = safe_malloc(ur->nrops, *ur->hss_of_ops);
-        int count = 0;
-        cinstr = -1;
-        while (get_next_unique_instr(&cinstr, set))
-                ur->hss_of_ops[count++] = set->hss_of_new[set->instr[cinstr].instr[2]];
-        ur->operators = safe_malloc(ur->nrops, *ur->operators);
-        for (int i = 0; i < ur->nrops; ++i) {
-                const int chss = ur->hss_of_ops[i];
-                init_sparseblocks(&ur->operators[i], tmpbb[chss],
-                                  rOperators_give_nr_blocks_for_hss(ur, chss), 'c');
-        }
-        for (int i = 0; i < ur->nrhss; ++i) safe_free(tmpbb[i]);
-        safe_free(tmpbb);
-}
-
 void rOperators_append_phys(struct rOperators *newrops, const struct rOperators *oldrops)
 {
         const struct rOperators *or = oldrops;
@@ -359,7 +296,7 @@ void rOperators_append_phys(struct rOperators *newrops, const struct rOperators 
         int bonds[3];
         get_bonds_of_site(site, bonds);
         struct rOperators ur;
-        pa_init_unique(&ur, bonds[2 * or->is_left], or->is_left, &set);
+        dropin_init_unique(&ur, bonds[2 * or->is_left], or->is_left, true, &set);
 
         /* the unique instructions with their MPO sectors (compress_instructions) */
         struct pa_ops *ci = safe_malloc(set.nr_instr + 1, struct pa_ops);
@@ -393,17 +330,11 @@ void rOperators_append_phys(struct rOperators *newrops, const struct rOperators 
         b2[2] = get_hamiltonianbond(or->bond);
         get_symsecs_arr(3, oss, b2);
 
-        /* element bases */
-        int64_t *obase = safe_malloc(or->nrops + 1, int64_t);
-        int64_t *ubase = safe_malloc(ur.nrops + 1, int64_t);
-        obase[0] = ubase[0] = 0;
-        for (int i = 0; i < or->nrops; ++i)
-                obase[i + 1] = obase[i] + or->operators[i].beginblock[nblocks_in_operator(or, i)];
-        for (int i = 0; i < ur.nrops; ++i)
-                ubase[i + 1] = ubase[i] + ur.operators[i].beginblock[nblocks_in_operator(&ur, i)];
+        int64_t *obase = dropin_op_bases(or);
+        int64_t *ubase = dropin_op_bases(&ur);
 
-        struct pu_vec dst = {0, 0, 0, sizeof(int64_t)}, src = {0, 0, 0, sizeof(int64_t)};
-        struct pu_vec len = {0, 0, 0, sizeof(int)}, scl = {0, 0, 0, sizeof(double)};
+        struct dv_vec dst = {0, 0, 0, sizeof(int64_t)}, src = {0, 0, 0, sizeof(int64_t)};
+        struct dv_vec len = {0, 0, 0, sizeof(int)}, scl = {0, 0, 0, sizeof(double)};
         const int N = ur.begin_blocks_of_hss[ur.nrhss];
         for (int usb = 0; usb < N; ++usb) {
                 const QN_TYPE *uqn = &ur.qnumbers[usb * 3];
@@ -440,33 +371,26 @@ void rOperators_append_phys(struct rOperators *newrops, const struct rOperators 
                                 const double site_el = pref * el_siteop(ci[i].so, ids[0][1], ids[1][1]);
                                 const int64_t d0 = ubase[i] + ur.operators[i].beginblock[ublock];
                                 const int64_t s0 = obase[ci[i].po] + ob->beginblock[oblock];
-                                pu_push(&dst, &d0);
-                                pu_push(&src, &s0);
-                                pu_push(&len, &n);
-                                pu_push(&scl, &site_el);
+                                dv_push(&dst, &d0);
+                                dv_push(&src, &s0);
+                                dv_push(&len, &n);
+                                dv_push(&scl, &site_el);
                         }
                 }
                 safe_free(prods);
         }
 
-        double *src_tel = safe_malloc(obase[or->nrops] + 1, double);
+        double *src_tel = dropin_gather(or, obase);
         double *dst_tel = safe_malloc(ubase[ur.nrops] + 1, double);
-        for (int i = 0; i < or->nrops; ++i)
-                if (obase[i + 1] > obase[i])
-                        memcpy(src_tel + obase[i], or->operators[i].tel,
-                               sizeof(double) * (size_t) (obase[i + 1] - obase[i]));
         t3ns_scalecopy_desc d = {(int) scl.n, dst.a, src.a, len.a, scl.a, obase[or->nrops],
                                  ubase[ur.nrops]};
         if (t3ns_scalecopy_host(&d, src_tel, dst_tel) != T3NS_OK) {
                 fprintf(stderr, "t3ns drop-in: rOperators_append_phys: %s\n", t3ns_last_error());
                 exit(EXIT_FAILURE);
         }
-        for (int i = 0; i < ur.nrops; ++i)
-                if (ubase[i + 1] > ubase[i])
-                        memcpy(ur.operators[i].tel, dst_tel + ubase[i],
-                               sizeof(double) * (size_t) (ubase[i + 1] - ubase[i]));
+        dropin_scatter(&ur, ubase, dst_tel);
         *newrops = sum_unique_rOperators(&ur, &set);
-        destroy_rOperators(&ur);
+        destroy_rOperators(&ur);   /* `set` is the reference's cached set: not ours to free */
         safe_free(src_tel);
         safe_free(dst_tel);
         safe_free(obase);

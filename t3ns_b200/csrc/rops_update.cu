@@ -4,6 +4,13 @@
 // src/rOperators_pUpdate.c:665-673): scaled copies of whole blocks, one CTA
 // per block.
 //
+// Branching update (reference update_rOperators_branching,
+// src/rOperators_bUpdate.c:229-248): per (new block, O1 block, O2 block,
+// site-tensor block, bra block) entry and instruction, O1 and O2 are applied
+// to the site-tensor block on their axes and the result is contracted with
+// the bra block over both (update_selected_blocks, :1043-1072); a CTA owns a
+// new block, intermediates in a per-CTA scratch slice.
+//
 // Physical update (reference update_rOperators_physical,
 // src/rOperators_pUpdate.c:364-387): for every updated block and every
 // original block that maps onto it (pUpdate_block, :323-362), all operators
@@ -78,6 +85,88 @@ __global__ void scalecopy_kernel(int n, const int64_t *__restrict__ dst_off,
                 const double *a = src + src_off[e];
                 double *b = dst + dst_off[e];
                 for (int j = threadIdx.x; j < len[e]; j += blockDim.x) b[j] = s * a[j];
+        }
+}
+
+// out = op (r x s, column-major) applied on axis ax of in (dims w, w[ax] = s)
+__device__ void apply_axis_dmma(int ax, const int *w, int r, const double *op, const double *in,
+                                double *out)
+{
+        if (ax == 0) {
+                cta_dgemm<false, false>(r, w[1] * w[2], w[0], 1.0, op, r, in, w[0], 0.0, out, r);
+        } else if (ax == 1) {
+                // slices along axis 2 are independent outputs (no barrier needed)
+                for (int c = 0; c < w[2]; ++c)
+                        cta_dgemm<false, true>(w[0], r, w[1], 1.0, in + (int64_t) c * w[0] * w[1], w[0],
+                                               op, r, 0.0, out + (int64_t) c * w[0] * r, w[0]);
+        } else {
+                cta_dgemm<false, true>(w[0] * w[1], r, w[2], 1.0, in, (int64_t) w[0] * w[1], op, r,
+                                       0.0, out, (int64_t) w[0] * w[1]);
+        }
+}
+
+// Branching update: for every entry of a unit (one new block) and every op
+// triple of the entry, W1 = O1 on axis a of T, W2 = O2 on axis b of W1,
+// New += pref * contraction of Ta and W2 over axes a and b.
+__global__ void __launch_bounds__(kUpdThreads)
+bupdate_kernel(int3 ax, int nunits, const int *__restrict__ unit_ptr,
+               const int *__restrict__ dims, const int64_t *__restrict__ t_off,
+               const int64_t *__restrict__ ta_off, const double *__restrict__ pref,
+               const int *__restrict__ op_ptr, const int64_t *__restrict__ o1_off,
+               const int64_t *__restrict__ o2_off, const int64_t *__restrict__ new_off,
+               const double *__restrict__ T, const double *__restrict__ O1,
+               const double *__restrict__ O2, double *NEW, double *scratch, int64_t w1cap,
+               int64_t w2cap, int *counter)
+{
+        __shared__ int unit;
+        double *W1 = scratch + (int64_t) blockIdx.x * (w1cap + w2cap);
+        double *W2 = W1 + w1cap;
+        const int a = ax.x, b = ax.y, g = ax.z;
+        for (;;) {
+                if (threadIdx.x == 0) unit = atomicAdd(counter, 1);
+                __syncthreads();
+                const int u = unit;
+                __syncthreads();
+                if (u >= nunits) break;
+                for (int e = unit_ptr[u]; e < unit_ptr[u + 1]; ++e) {
+                        const int kd[3] = {dims[6 * e], dims[6 * e + 1], dims[6 * e + 2]};
+                        const int bd[3] = {dims[6 * e + 3], dims[6 * e + 4], dims[6 * e + 5]};
+                        const double *Tk = T + t_off[e];
+                        const double *Tb = T + ta_off[e];
+                        const double pf = pref[e];
+                        // cheaper of the two orders (the results differ by rounding only)
+                        const bool a_first = (int64_t) kd[b] * bd[a] * (kd[a] + bd[b]) <=
+                                             (int64_t) kd[a] * bd[b] * (kd[b] + bd[a]);
+                        const int x1 = a_first ? a : b, x2 = a_first ? b : a;
+                        int v1[3] = {kd[0], kd[1], kd[2]};
+                        v1[x1] = bd[x1];
+                        for (int p = op_ptr[e]; p < op_ptr[e + 1]; ++p) {
+                                const double *P1 = a_first ? O1 + o1_off[p] : O2 + o2_off[p];
+                                const double *P2 = a_first ? O2 + o2_off[p] : O1 + o1_off[p];
+                                apply_axis_dmma(x1, kd, bd[x1], P1, Tk, W1);
+                                __syncthreads();
+                                apply_axis_dmma(x2, v1, bd[x2], P2, W1, W2);
+                                __syncthreads();
+                                double *Nw = NEW + new_off[p];
+                                // New (bd[g] x kd[g]) += pf * sum over axes a, b of Tb * W2
+                                if (g == 2) {
+                                        const int R = bd[0] * bd[1];
+                                        cta_dgemm<true, false>(bd[2], kd[2], R, pf, Tb, R, W2, R, 1.0, Nw, bd[2]);
+                                } else if (g == 0) {
+                                        const int R = bd[1] * bd[2];
+                                        cta_dgemm<false, true>(bd[0], kd[0], R, pf, Tb, bd[0], W2, kd[0], 1.0,
+                                                               Nw, bd[0]);
+                                } else {
+                                        // the same warp owns the same output tile in every slice
+                                        for (int c = 0; c < bd[2]; ++c)
+                                                cta_dgemm<true, false>(bd[1], kd[1], bd[0], pf,
+                                                                       Tb + (int64_t) c * bd[0] * bd[1], bd[0],
+                                                                       W2 + (int64_t) c * bd[0] * kd[1], bd[0],
+                                                                       1.0, Nw, bd[1]);
+                                }
+                                __syncthreads();
+                        }
+                }
         }
 }
 
@@ -195,7 +284,89 @@ int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst)
         return T3NS_OK;
 }
 
+int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o1_tel,
+                const double *o2_tel, double *new_tel)
+{
+        if (!d || !new_tel || d->nunits < 0 || d->nentries < 0)
+                return set_error(T3NS_E_ARG, "bupdate: bad descriptor");
+        const int a = d->ax[0], b = d->ax[1], g = d->ax[2];
+        if (a < 0 || a > 2 || b < 0 || b > 2 || g < 0 || g > 2 || a == b || a == g || b == g)
+                return set_error(T3NS_E_ARG, "bupdate: axes are not a permutation");
+        const int ntr = d->nentries ? d->op_ptr[d->nentries] : 0;
+        int64_t w1cap = 1, w2cap = 1;
+        for (int e = 0; e < d->nentries; ++e) {
+                const int *kd = d->dims + 6 * e, *bd = kd + 3;
+                for (int j = 0; j < 6; ++j)
+                        if (kd[j] < 0) return set_error(T3NS_E_ARG, "bupdate: negative dims");
+                int64_t tk = (int64_t) kd[0] * kd[1] * kd[2], tb = (int64_t) bd[0] * bd[1] * bd[2];
+                if (d->t_off[e] < 0 || d->t_off[e] + tk > d->t_elems || d->ta_off[e] < 0 ||
+                    d->ta_off[e] + tb > d->t_elems)
+                        return set_error(T3NS_E_ARG, "bupdate: site-tensor block out of range");
+                // either order of the two operator applications may be taken
+                auto one_applied = [&](int x) {
+                        int64_t v = bd[x];
+                        for (int i = 0; i < 3; ++i)
+                                if (i != x) v *= kd[i];
+                        return v;
+                };
+                w1cap = std::max(w1cap, std::max(one_applied(a), one_applied(b)));
+                w2cap = std::max(w2cap, (int64_t) bd[a] * bd[b] * kd[g]);
+                for (int p = d->op_ptr[e]; p < d->op_ptr[e + 1]; ++p)
+                        if (d->o1_off[p] < 0 || d->o1_off[p] + (int64_t) bd[a] * kd[a] > d->o1_elems ||
+                            d->o2_off[p] < 0 || d->o2_off[p] + (int64_t) bd[b] * kd[b] > d->o2_elems ||
+                            d->new_off[p] < 0 || d->new_off[p] + (int64_t) bd[g] * kd[g] > d->new_elems)
+                                return set_error(T3NS_E_ARG, "bupdate: operator block out of range");
+        }
+        for (int u = 0; u < d->nunits; ++u)
+                if (d->unit_ptr[u] > d->unit_ptr[u + 1] || d->unit_ptr[u + 1] > d->nentries)
+                        return set_error(T3NS_E_ARG, "bupdate: unit list out of range");
+        w1cap = (w1cap + 31) / 32 * 32;
+        w2cap = (w2cap + 31) / 32 * 32;
+        Allocs al;
+        int *unit_ptr, *op_ptr, *dims, *counter;
+        int64_t *t_off, *ta_off, *o1_off, *o2_off, *new_off;
+        double *pref, *T, *O1, *O2, *NEW, *scratch;
+        T3NS_TRY(upload(al.v, &unit_ptr, d->unit_ptr, d->nunits + 1));
+        T3NS_TRY(upload(al.v, &op_ptr, d->op_ptr, d->nentries + 1));
+        T3NS_TRY(upload(al.v, &dims, d->dims, (size_t) 6 * d->nentries));
+        T3NS_TRY(upload(al.v, &t_off, d->t_off, d->nentries));
+        T3NS_TRY(upload(al.v, &ta_off, d->ta_off, d->nentries));
+        T3NS_TRY(upload(al.v, &pref, d->pref, d->nentries));
+        T3NS_TRY(upload(al.v, &o1_off, d->o1_off, ntr));
+        T3NS_TRY(upload(al.v, &o2_off, d->o2_off, ntr));
+        T3NS_TRY(upload(al.v, &new_off, d->new_off, ntr));
+        T3NS_TRY(upload(al.v, &T, t_tel, d->t_elems));
+        T3NS_TRY(upload(al.v, &O1, o1_tel, d->o1_elems));
+        T3NS_TRY(upload(al.v, &O2, o2_tel, d->o2_elems));
+        T3NS_TRY(upload<double>(al.v, &NEW, nullptr, d->new_elems));
+        T3NS_TRY(upload<int>(al.v, &counter, nullptr, 1));
+        int dev = 0, sms = 148;
+        T3NS_CUDA_TRY(cudaGetDevice(&dev));
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int grid = std::max(1, std::min(d->nunits, 4 * sms));
+        T3NS_TRY(upload<double>(al.v, &scratch, nullptr, (size_t) grid * (w1cap + w2cap)));
+        T3NS_CUDA_TRY(cudaMemset(NEW, 0, sizeof(double) * std::max<int64_t>(d->new_elems, 1)));
+        T3NS_CUDA_TRY(cudaMemset(counter, 0, sizeof(int)));
+        if (d->nunits > 0) {
+                bupdate_kernel<<<grid, kUpdThreads>>>(make_int3(a, b, g), d->nunits, unit_ptr, dims,
+                                                      t_off, ta_off, pref, op_ptr, o1_off, o2_off,
+                                                      new_off, T, O1, O2, NEW, scratch, w1cap, w2cap,
+                                                      counter);
+                T3NS_CUDA_TRY(cudaGetLastError());
+        }
+        if (d->new_elems)
+                T3NS_CUDA_TRY(cudaMemcpy(new_tel, NEW, sizeof(double) * d->new_elems,
+                                         cudaMemcpyDeviceToHost));
+        return T3NS_OK;
+}
+
 }  // namespace t3ns
+
+extern "C" int t3ns_bupdate_host(const t3ns_bupdate_desc *d, const double *t_tel,
+                                 const double *o1_tel, const double *o2_tel, double *new_tel)
+{
+        return t3ns::bupdate_run(d, t_tel, o1_tel, o2_tel, new_tel);
+}
 
 extern "C" int t3ns_scalecopy_host(const t3ns_scalecopy_desc *d, const double *src, double *dst)
 {

@@ -26,11 +26,12 @@ def captured_steps(max_bytes=400 << 20):
     return out
 
 
-def pupdate_captures():
-    """Physical-update captures with their compiled schedules."""
+def pupdate_captures(kind="pupdate"):
+    """Renormalised-operator update captures with their compiled schedules:
+    kind "pupdate" (physical) or "bupdate" (branching)."""
     out = []
     for p in sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "captures", "pupdate_*",
-                                           "pupdate_*.t3c"))):
+                                           f"{kind}_*.t3c"))):
         if os.path.exists(p.replace(".t3c", ".sched")):
             out.append(p)
     return out

@@ -1,8 +1,10 @@
 """Helpers to replay captured renormalised-operator updates: build the
-engine descriptor from a compiled schedule ("pu.*" records), emulate it on
-the CPU (numpy) or run it through the C ABI, apply the reference's zero-block
-removal (kick_zero_blocks, src/sparseblocks.c:73-107) and compare with the
-reference's output captured in the same file ("ops1.*" records)."""
+engine descriptor from a compiled schedule ("pu.*" records for the physical
+update, "bu.*" for the branching one), emulate it on the CPU (numpy) or run
+it through the C ABI, sum unique operators as the reference does, apply the
+reference's zero-block removal (kick_zero_blocks, src/sparseblocks.c:73-107)
+and compare with the reference's output captured in the same file ("ops1.*"
+records for the physical update, "ops2.*" for the branching one)."""
 import ctypes as C
 
 import numpy as np
@@ -78,22 +80,21 @@ def run_pupdate_gpu(rec, sch):
     return new[:d.new_elems]
 
 
-def kick_and_compare(rec, sch, new):
+def kick_compare(rec, idx, pre):
     """Apply zero-block removal (a block whose elements are all below 1e-20
-    in magnitude is dropped) to `new` operator by operator and compare with
-    the reference output: same surviving blocks, elements equal to the given
-    relative tolerance.  Returns the largest element difference relative to
-    the largest reference element."""
-    begins, ref = ops_structure(rec, 1)
-    pre = sch["pu.new_beginblock"].astype(np.int64)
-    base = sch["pu.new_base"].astype(np.int64)
+    in magnitude is dropped) to the operators `pre` -- a list of (begin array
+    before removal, elements) per operator -- and compare with the
+    reference's operator set `idx` of the capture: same surviving blocks,
+    elements compared relative to the largest reference element.  Returns
+    that largest relative difference."""
+    begins, ref = ops_structure(rec, idx)
+    assert len(begins) == len(pre)
     scale = max(np.abs(ref).max() if ref.size else 0.0, 1e-300)
-    worst, roff, poff = 0.0, 0, 0
+    worst, roff = 0.0, 0
     for k, bb in enumerate(begins):
         nb = len(bb) - 1
-        pbb = pre[poff:poff + nb + 1]
-        poff += nb + 1
-        seg = new[int(base[k]):int(base[k + 1])]
+        pbb, seg = pre[k]
+        assert len(pbb) == nb + 1, (k, len(pbb), nb)
         rseg = ref[roff:roff + int(bb[-1])]
         roff += int(bb[-1])
         for b in range(nb):
@@ -104,3 +105,114 @@ def kick_and_compare(rec, sch, new):
             if rsz:
                 worst = max(worst, float(np.abs(blk - rseg[bb[b]:bb[b + 1]]).max()) / scale)
     return worst
+
+
+def _nblocks(rec, idx, hss):
+    bbh = rec[f"ops{idx}.begin_blocks_of_hss"]
+    return int(bbh[hss + 1] - bbh[hss])
+
+
+def kick_and_compare(rec, sch, new):
+    """kick_compare for a physical update: `new` is the updated set's
+    concatenated elements in the schedule's layout."""
+    pre = sch["pu.new_beginblock"].astype(np.int64)
+    base = sch["pu.new_base"].astype(np.int64)
+    out, poff = [], 0
+    for k, h in enumerate(rec["ops1.hss_of_ops"]):
+        n = _nblocks(rec, 1, int(h))
+        out.append((pre[poff:poff + n + 1], new[int(base[k]):int(base[k + 1])]))
+        poff += n + 1
+    return kick_compare(rec, 1, out)
+
+
+class BupdateDesc(C.Structure):
+    _fields_ = [("ax", C.c_int * 3), ("nunits", C.c_int), ("unit_ptr", C.c_void_p),
+                ("nentries", C.c_int), ("dims", C.c_void_p), ("t_off", C.c_void_p),
+                ("ta_off", C.c_void_p), ("pref", C.c_void_p), ("op_ptr", C.c_void_p),
+                ("o1_off", C.c_void_p), ("o2_off", C.c_void_p), ("new_off", C.c_void_p),
+                ("t_elems", C.c_int64), ("o1_elems", C.c_int64), ("o2_elems", C.c_int64),
+                ("new_elems", C.c_int64)]
+
+
+def _block3(arr, off, d):
+    """Column-major block of dims d as an array indexed [i0, i1, i2]."""
+    n = d[0] * d[1] * d[2]
+    return arr[off:off + n].reshape(d[2], d[1], d[0]).transpose(2, 1, 0)
+
+
+def _block2(arr, off, r, c):
+    return arr[off:off + r * c].reshape(c, r).T
+
+
+def emulate_bupdate(rec, sch):
+    """numpy replay of a compiled branching-update schedule: the unique
+    operators' concatenated elements."""
+    T, O1, O2 = rec["T.tel"], rec["ops0.tel"], rec["ops1.tel"]
+    a, b, g = (int(v) for v in sch["bu.ax"])
+    new = np.zeros(int(sch["bu.unique_base"][-1]))
+    dims = sch["bu.dims"].reshape(-1, 6)
+    bra, ket = "abc", "xyz"
+    spec = (f"{bra},{ket},{bra[a]}{ket[a]},{bra[b]}{ket[b]}->{bra[g]}{ket[g]}")
+    for e in range(len(sch["bu.pref"])):
+        kd, bd = [int(v) for v in dims[e, :3]], [int(v) for v in dims[e, 3:]]
+        Tk = _block3(T, int(sch["bu.t_off"][e]), kd)
+        Tb = _block3(T, int(sch["bu.ta_off"][e]), bd)
+        for p in range(sch["bu.op_ptr"][e], sch["bu.op_ptr"][e + 1]):
+            A = _block2(O1, int(sch["bu.o1_off"][p]), bd[a], kd[a])
+            B = _block2(O2, int(sch["bu.o2_off"][p]), bd[b], kd[b])
+            U = sch["bu.pref"][e] * np.einsum(spec, Tb, Tk, A, B, optimize=True)
+            n = int(sch["bu.new_off"][p])
+            new[n:n + U.size] += U.T.reshape(-1)
+    return new
+
+
+def run_bupdate_gpu(rec, sch):
+    lib = native.load()
+    lib.t3ns_bupdate_host.argtypes = [C.POINTER(BupdateDesc), C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+    keep = {k: np.ascontiguousarray(sch[k]) for k in sch}
+    d = BupdateDesc()
+    for i in range(3):
+        d.ax[i] = int(keep["bu.ax"][i])
+    d.nunits = len(keep["bu.unit_ptr"]) - 1
+    d.unit_ptr = keep["bu.unit_ptr"].ctypes.data
+    d.nentries = len(keep["bu.pref"])
+    for f in ("dims", "t_off", "ta_off", "pref", "op_ptr", "o1_off", "o2_off", "new_off"):
+        setattr(d, f, keep["bu." + f].ctypes.data)
+    T = np.ascontiguousarray(rec["T.tel"])
+    o1 = np.ascontiguousarray(rec["ops0.tel"])
+    o2 = np.ascontiguousarray(rec["ops1.tel"])
+    d.t_elems, d.o1_elems, d.o2_elems = T.size, o1.size, o2.size
+    d.new_elems = int(keep["bu.unique_base"][-1])
+    new = np.empty(max(d.new_elems, 1))
+    native.check(lib.t3ns_bupdate_host(C.byref(d), T.ctypes.data, o1.ctypes.data,
+                                       o2.ctypes.data, new.ctypes.data), "bupdate_host")
+    return new[:d.new_elems]
+
+
+def sum_unique(rec, sch, unique):
+    """The reference's sum_unique_rOperators (src/rOperators_init.c:228-265)
+    on the unique operators: new operator k = sum of instr.pref times the
+    unique operator of every instruction that writes k.  Returns the
+    (begin array, elements) of every new operator before zero-block removal;
+    the block counts per MPO sector come from the captured result (ops2)."""
+    ubase = sch["bu.unique_base"].astype(np.int64)
+    uhss = sch["bu.unique_hss"]
+    ubb = sch["bu.unique_beginblock"].astype(np.int64)
+    begins, off = [], 0
+    for u in range(len(uhss)):
+        n = _nblocks(rec, 2, int(uhss[u]))
+        begins.append(ubb[off:off + n + 1])
+        off += n + 1
+    hss_new = sch["bu.hss_of_new"]
+    instr = sch["bu.instr"].reshape(-1, 3)
+    out = []
+    for k in range(len(hss_new)):
+        # layout of any unique operator of the same MPO sector
+        u0 = int(np.flatnonzero(uhss == hss_new[k])[0])
+        acc = np.zeros(int(begins[u0][-1]))
+        for i in np.flatnonzero(instr[:, 2] == k):
+            u = int(sch["bu.instr_unique"][i])
+            acc += sch["bu.instr_pref"][i] * unique[int(ubase[u]):int(ubase[u + 1])]
+        out.append((begins[u0], acc))
+    return out
