@@ -240,6 +240,20 @@ typedef struct {
 int t3ns_bupdate_host(const t3ns_bupdate_desc *d, const double *t_tel, const double *o1_tel,
                       const double *o2_tel, double *new_tel);
 
+/* Dense FP64 factorisations of one symmetry sector of the site-tensor
+ * decomposition, on host column-major arrays, with LAPACK's argument
+ * meaning.  They replace the reference's LAPACKE_dgesdd ('S' and 'N'),
+ * LAPACKE_dgeqrf and LAPACKE_dorgqr calls (src/siteTensor_decompose.c:1060,
+ * :565, :285, :295).  Safe to call from several host threads at once (each
+ * thread has its own stream).  t3ns_gesdd_host returns T3NS_E_EIG when the
+ * Jacobi sweeps do not converge; singular values come out descending, and
+ * singular vectors are unique up to sign (and rotation within a degenerate
+ * singular value), as LAPACK's are. */
+int t3ns_gesdd_host(char jobz, int m, int n, const double *a, int lda, double *s, double *u,
+                    int ldu, double *vt, int ldvt);
+int t3ns_geqrf_host(int m, int n, double *a, int lda, double *tau);
+int t3ns_orgqr_host(int m, int n, int k, double *a, int lda, const double *tau);
+
 /* Largest vector t3ns_precondition_device_noalloc accepts (elements). */
 #define T3NS_NOALLOC_MAX_SIZE 16777216LL
 

@@ -4,7 +4,8 @@
  * These are exactly the declarations of the reference's own headers, so the
  * reference's unchanged sweep driver links against libt3ns_dropin.so in place
  * of the reference objects Heff.o, davidson.o, wrapper_solvers.o,
- * rOperators_pUpdate.o and rOperators_bUpdate.o.  The
+ * rOperators_pUpdate.o and rOperators_bUpdate.o, and ahead of the LAPACK
+ * library for the decomposition's factorisations.  The
  * structs are the reference's (include/Heff.h, include/rOperators.h,
  * include/siteTensor.h); the library is compiled against those headers
  * because the driver allocates struct Heffdata itself.  All arithmetic runs
@@ -75,6 +76,17 @@ void rOperators_append_phys(struct rOperators *newrops, const struct rOperators 
  * of the branching tensor tens, built from Operator[0] and Operator[1]. */
 void update_rOperators_branching(struct rOperators *newops, const struct rOperators *Operator,
                                  const struct siteTensor *tens);
+
+/* Replace the LAPACKE entry points through which the reference's site-tensor
+ * decomposition factorises each symmetry sector (src/siteTensor_decompose.c:
+ * LAPACKE_dgesdd at :1060 and :565, LAPACKE_dgeqrf at :285, LAPACKE_dorgqr at
+ * :295; LAPACKE's own declarations, column-major layout only).  Link
+ * libt3ns_dropin.so ahead of the BLAS/LAPACK library.  Return LAPACK's info
+ * codes (0, -i for a bad argument, 1 when the SVD did not converge). */
+int LAPACKE_dgesdd(int layout, char jobz, int m, int n, double *a, int lda, double *s, double *u,
+                   int ldu, double *vt, int ldvt);
+int LAPACKE_dgeqrf(int layout, int m, int n, double *a, int lda, double *tau);
+int LAPACKE_dorgqr(int layout, int m, int n, int k, double *a, int lda, const double *tau);
 
 /* Test hook (no counterpart in the reference): writes the compiled schedule
  * of *data to `path` in the step-file layout without using the GPU. */

@@ -174,6 +174,27 @@ def ensure_updates(threads=None):
                            "--schedule-lib", lib], threads, steps=False)
 
 
+def ensure_dense(threads=None):
+    """Dense-factorisation captures: the LAPACKE_dgesdd / dgeqrf / dorgqr
+    calls of the site-tensor decomposition with the reference LAPACK's
+    outputs, over one sweep of the Hubbard and QC12 cases (the first calls
+    of each run; the calls come from OpenMP threads, so their numbering is
+    not deterministic)."""
+    threads = threads or os.cpu_count() or 1
+    for name, args in [
+        ("dense_hub10", ["--net", os.path.join(NETS, "t3ns_10.netw"), "--inter",
+                         "NN_HUBBARD ( t = 1 U = 4 )", "--symm", "Z2,U1,SU2", "--ts", "0,10,0",
+                         "--regime", "128,128,0,2,1e-5,100,1,1e-8,0"]),
+        ("dense_qc12", ["--net", os.path.join(NETS, "t3ns_12.netw"), "--inter", _fcidump(12),
+                        "--symm", "Z2,U1,SU2", "--ts", "0,12,0",
+                        "--regime", "64,64,0,2,1e-5,100,1,1e-8,0"])]:
+        d = os.path.join(REF, "captures", name)
+        if os.path.exists(os.path.join(d, "run.log")):
+            continue
+        _capture(d, args, ["--capture-dense", d, "--capture-dense-limit", "80"], threads,
+                 steps=False)
+
+
 def ensure_d512(threads=None):
     threads = threads or os.cpu_count() or 1
     d = os.path.join(REF, "captures", "qc24_D512")
@@ -198,6 +219,9 @@ if __name__ == "__main__":
         sys.exit(0)
     if sys.argv[1] == "updates":
         ensure_updates()
+        sys.exit(0)
+    if sys.argv[1] == "dense":
+        ensure_dense()
         sys.exit(0)
     if sys.argv[1] == "d512":
         ensure_d512()

@@ -21,6 +21,7 @@
  */
 #define _GNU_SOURCE
 #include <dlfcn.h>
+#include <pthread.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -45,16 +46,21 @@
 
 static FILE *cap_fp;
 
-static void cap_put(const char *name, int dtype, int64_t count, const void *data)
+static void cap_put_f(FILE *f, const char *name, int dtype, int64_t count, const void *data)
 {
         char nm[48] = {0};
         strncpy(nm, name, sizeof nm - 1);
         int32_t hdr[2] = {dtype, 0};
-        fwrite(nm, 1, sizeof nm, cap_fp);
-        fwrite(hdr, sizeof hdr, 1, cap_fp);
-        fwrite(&count, sizeof count, 1, cap_fp);
+        fwrite(nm, 1, sizeof nm, f);
+        fwrite(hdr, sizeof hdr, 1, f);
+        fwrite(&count, sizeof count, 1, f);
         const size_t el = dtype == 1 ? 4 : 8;
-        if (count > 0) fwrite(data, el, (size_t) count, cap_fp);
+        if (count > 0) fwrite(data, el, (size_t) count, f);
+}
+
+static void cap_put(const char *name, int dtype, int64_t count, const void *data)
+{
+        cap_put_f(cap_fp, name, dtype, count, data);
 }
 
 static void cap_i32(const char *name, int64_t n, const int *d) { cap_put(name, 1, n, d); }
@@ -75,6 +81,8 @@ static int opt_capture_nvec = 2;         /* seeded matvec pairs         */
 static int opt_capture_noeig;            /* skip Davidson in capture    */
 static const char *opt_schedule_lib;     /* drop-in whose schedule to dump */
 static const char *opt_capture_pupdate;  /* dir for physical-update captures */
+static const char *opt_capture_dense;    /* dir for dense LAPACK call captures */
+static int opt_dense_limit = 400;
 static int opt_pupdate_limit = 4;
 static int opt_pupdate_count;
 static int opt_step_counter;
@@ -433,6 +441,125 @@ void update_rOperators_branching(struct rOperators *newops, const struct rOperat
         }
 }
 
+/* Captures the dense factorisations of the site-tensor decomposition: every
+ * LAPACKE_dgesdd / dgeqrf / dorgqr call the reference makes
+ * (src/siteTensor_decompose.c:285, :295, :1060, :565) is logged with its
+ * sizes to dense_sizes.txt, and up to --capture-dense-limit calls of each
+ * kind are written with their inputs and the reference LAPACK's outputs.  The calls
+ * come from OpenMP threads, so the bookkeeping is under a mutex and every
+ * capture has its own file. */
+static pthread_mutex_t dense_mu = PTHREAD_MUTEX_INITIALIZER;
+static int dense_count[3];   /* per kind: gesdd, geqrf, orgqr */
+
+static FILE *dense_open(const char *kind, int m, int n, int k)
+{
+        if (!opt_capture_dense) return NULL;
+        char path[4096];
+        const int kid = kind[2] == 's' ? 0 : kind[2] == 'q' ? 1 : 2;
+        pthread_mutex_lock(&dense_mu);
+        const int idx = dense_count[kid]++;
+        snprintf(path, sizeof path, "%s/dense_sizes.txt", opt_capture_dense);
+        FILE *log = fopen(path, "a");
+        if (log) {
+                fprintf(log, "%s %d %d %d\n", kind, m, n, k);
+                fclose(log);
+        }
+        pthread_mutex_unlock(&dense_mu);
+        if (idx >= opt_dense_limit) return NULL;
+        snprintf(path, sizeof path, "%s/%s_%05d.t3c", opt_capture_dense, kind, idx);
+        FILE *f = fopen(path, "wb");
+        if (f) fwrite("T3NSCAP1", 1, 8, f);
+        return f;
+}
+
+/* column-major m x n with leading dimension ld, compacted */
+static double *dense_copy(const double *a, int m, int n, int ld)
+{
+        double *c = malloc(sizeof *c * (size_t) (m > 0 && n > 0 ? m * n : 1));
+        for (int j = 0; j < n; ++j)
+                for (int i = 0; i < m; ++i) c[i + (size_t) j * m] = a[i + (size_t) j * ld];
+        return c;
+}
+
+static void dense_put_mat(FILE *f, const char *nm, const double *a, int m, int n, int ld)
+{
+        double *c = dense_copy(a, m, n, ld);
+        cap_put_f(f, nm, 3, (int64_t) m * n, c);
+        free(c);
+}
+
+static void dense_put_int(FILE *f, const char *nm, int v) { cap_put_f(f, nm, 1, 1, &v); }
+
+typedef int (*gesdd_fn)(int, char, int, int, double *, int, double *, double *, int, double *, int);
+int LAPACKE_dgesdd(int layout, char jobz, int m, int n, double *a, int lda, double *s,
+                   double *u, int ldu, double *vt, int ldvt)
+{
+        static gesdd_fn real;
+        if (!real) real = (gesdd_fn) dlsym(RTLD_NEXT, "LAPACKE_dgesdd");
+        const int mn = m < n ? m : n;
+        FILE *f = dense_open("gesdd", m, n, jobz);
+        if (f) {
+                dense_put_int(f, "gesdd.m", m);
+                dense_put_int(f, "gesdd.n", n);
+                dense_put_int(f, "gesdd.jobz", jobz);
+                dense_put_mat(f, "gesdd.a", a, m, n, lda);
+        }
+        const int info = real(layout, jobz, m, n, a, lda, s, u, ldu, vt, ldvt);
+        if (f) {
+                dense_put_int(f, "gesdd.info", info);
+                cap_put_f(f, "gesdd.s", 3, mn, s);
+                if (jobz == 'S') {
+                        dense_put_mat(f, "gesdd.u", u, m, mn, ldu);
+                        dense_put_mat(f, "gesdd.vt", vt, mn, n, ldvt);
+                }
+                fclose(f);
+        }
+        return info;
+}
+
+typedef int (*geqrf_fn)(int, int, int, double *, int, double *);
+int LAPACKE_dgeqrf(int layout, int m, int n, double *a, int lda, double *tau)
+{
+        static geqrf_fn real;
+        if (!real) real = (geqrf_fn) dlsym(RTLD_NEXT, "LAPACKE_dgeqrf");
+        FILE *f = dense_open("geqrf", m, n, 0);
+        if (f) {
+                dense_put_int(f, "geqrf.m", m);
+                dense_put_int(f, "geqrf.n", n);
+                dense_put_mat(f, "geqrf.a", a, m, n, lda);
+        }
+        const int info = real(layout, m, n, a, lda, tau);
+        if (f) {
+                dense_put_int(f, "geqrf.info", info);
+                dense_put_mat(f, "geqrf.qr", a, m, n, lda);
+                cap_put_f(f, "geqrf.tau", 3, m < n ? m : n, tau);
+                fclose(f);
+        }
+        return info;
+}
+
+typedef int (*orgqr_fn)(int, int, int, int, double *, int, const double *);
+int LAPACKE_dorgqr(int layout, int m, int n, int k, double *a, int lda, const double *tau)
+{
+        static orgqr_fn real;
+        if (!real) real = (orgqr_fn) dlsym(RTLD_NEXT, "LAPACKE_dorgqr");
+        FILE *f = dense_open("orgqr", m, n, k);
+        if (f) {
+                dense_put_int(f, "orgqr.m", m);
+                dense_put_int(f, "orgqr.n", n);
+                dense_put_int(f, "orgqr.k", k);
+                dense_put_mat(f, "orgqr.a", a, m, n, lda);
+                cap_put_f(f, "orgqr.tau", 3, k, tau);
+        }
+        const int info = real(layout, m, n, k, a, lda, tau);
+        if (f) {
+                dense_put_int(f, "orgqr.info", info);
+                dense_put_mat(f, "orgqr.q", a, m, n, lda);
+                fclose(f);
+        }
+        return info;
+}
+
 int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
                       int keep_deflate, double tol, int max_its,
                       const double *diagonal,
@@ -510,6 +637,8 @@ int main(int argc, char **argv)
                 else if (!strcmp(a, "--schedule-lib") && v) { opt_schedule_lib = v; ++i; }
                 else if (!strcmp(a, "--capture-pupdate") && v) { opt_capture_pupdate = v; ++i; }
                 else if (!strcmp(a, "--capture-pupdate-limit") && v) { opt_pupdate_limit = atoi(v); ++i; }
+                else if (!strcmp(a, "--capture-dense") && v) { opt_capture_dense = v; ++i; }
+                else if (!strcmp(a, "--capture-dense-limit") && v) { opt_dense_limit = atoi(v); ++i; }
                 else if (!strcmp(a, "--regime") && v) {
                         struct regime *r = &regs[nreg++];
                         memset(r, 0, sizeof *r);

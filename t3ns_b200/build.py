@@ -22,7 +22,8 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu", "precond_noalloc.cu", "rops_update.cu"]
+ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu", "precond_noalloc.cu", "rops_update.cu",
+                  "dense.cu"]
 
 
 def _run(cmd, cwd=None):
@@ -57,7 +58,7 @@ def build_engine(force: bool = False) -> str:
 
 REFERENCE_INCLUDE = os.environ.get("T3NS_REFERENCE_INCLUDE", "/root/reference/include")
 SHIM_INCLUDE = os.path.join(ROOT, "oracle", "shim")
-DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c", "bupdate_dropin.c"]
+DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c", "bupdate_dropin.c", "dense_dropin.c"]
 
 
 def build_dropin(force: bool = False):
