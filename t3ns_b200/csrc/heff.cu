@@ -18,10 +18,12 @@
 //   * the host flattens the schedule into one term per (pair, instruction)
 //     whose three operator blocks are all present (find_operator_tel,
 //     src/Heff.c:798-813), grouped by pair, pairs grouped by output block;
-//   * an output block becomes one or more work units, tiles along memory
-//     axes 1 and 2 small enough for a shared-memory accumulator; a tiled
-//     block's pairs contract the tiled axes first, so a tile's share of the
-//     work is exactly its rows of the last operators (no recomputation);
+//   * an output block becomes one or more work units, tiles along one or two
+//     memory axes small enough for a shared-memory accumulator; each tile
+//     applies only its own rows of every operator, and the tiling and each
+//     pair's contraction order are chosen together by their FLOPs summed over
+//     the tiles (a stage that runs before a tiled axis is contracted is
+//     repeated for every tile along that axis);
 //   * one persistent kernel; each CTA takes units off a global counter
 //     (heaviest first), keeps the unit's output tile in shared memory and
 //     walks its pairs.  A pair's terms share every block dimension and the
@@ -346,28 +348,38 @@ static const int kOrders3[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1},
                                    {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
 static const int kOrders2[2][2] = {{0, 1}, {1, 0}};
 
-// FLOPs of one term contracting axes in `seq` (memory axes) from dims `o`
-// to dims `n`, and the sizes of its first two intermediates for the tile
-// extents `ext` (equal to n on untiled axes).
+// FLOPs of contracting a pair in the order seq, summed over the tiles of
+// the output block: ext is the tile extent and nt the number of tiles along
+// each axis.  Each tile applies its own rows of every operator, so a stage
+// costs 2 * (new rows) * (old dim) * (the other current dims); an axis not
+// yet contracted is still at its old extent in every tile, so that stage is
+// repeated for every tile along it.  s1, s2: per-tile sizes of the first
+// two intermediates.
 static double seq_cost(const int *seq, int nst, const int *o, const int *n, const int *ext,
-                       int64_t *s1, int64_t *s2)
+                       const int *nt, int64_t *s1, int64_t *s2)
 {
         double fl = 0;
-        int64_t w[3] = {o[0], o[1], o[2]}, wt[3] = {o[0], o[1], o[2]};
+        bool done[3] = {false, false, false};
+        int64_t wt[3] = {o[0], o[1], o[2]};
         for (int s = 0; s < nst; ++s) {
-                fl += 2.0 * (double) w[0] * w[1] * w[2] * n[seq[s]];
-                w[seq[s]] = n[seq[s]];
-                wt[seq[s]] = ext[seq[s]];
+                const int a = seq[s];
+                double f = 2.0 * n[a] * o[a];
+                for (int j = 0; j < 3; ++j) {
+                        if (j == a) continue;
+                        f *= done[j] ? (double) n[j] : (double) o[j] * nt[j];
+                }
+                fl += f;
+                done[a] = true;
+                wt[a] = ext[a];
                 if (s == 0) *s1 = wt[0] * wt[1] * wt[2];
                 if (s == 1) *s2 = nst == 3 ? wt[0] * wt[1] * wt[2] : 0;
         }
         return fl;
 }
 
-// Cheapest contraction sequence for a pair whose first stages must be the
-// tiled axes (mask bit j: axis j is tiled), among those whose intermediates
-// fit the shared buffer.  Returns -1 if none fits.
-static int choose_seq(int nst, int tiled_mask, const int *o, const int *n, const int *ext,
+// Cheapest contraction sequence for a pair on a tiling (ext, nt) among those
+// whose intermediates fit the shared buffer.  Returns -1 if none fits.
+static int choose_seq(int nst, const int *o, const int *n, const int *ext, const int *nt,
                       double *fl_out, int seq_out[3])
 {
         static const int perms3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
@@ -378,16 +390,8 @@ static int choose_seq(int nst, int tiled_mask, const int *o, const int *n, const
         double bfl = 0;
         for (int q = 0; q < np; ++q) {
                 const int *seq = nst == 3 ? perms3[q] : perms2[q];
-                // tiled axes must come before every untiled axis
-                bool ok = true, seen_untiled = false;
-                for (int s = 0; s < nst; ++s) {
-                        const bool t = (tiled_mask >> seq[s]) & 1;
-                        if (t && seen_untiled) ok = false;
-                        if (!t) seen_untiled = true;
-                }
-                if (!ok) continue;
                 int64_t s1 = 0, s2 = 0;
-                const double fl = seq_cost(seq, nst, o, n, ext, &s1, &s2);
+                const double fl = seq_cost(seq, nst, o, n, ext, nt, &s1, &s2);
                 if (s1 + s2 > kWCap) continue;
                 if (best < 0 || fl < bfl) { best = q; bfl = fl; }
         }
@@ -564,16 +568,16 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 std::vector<int> best_seqs;
                 for (size_t ci = 0; ci < cand.size(); ++ci) {
                         const Cand &cd = cand[ci];
-                        const int mask = (cd.at < en[0] ? 1 : 0) | (cd.bt < en[1] ? 2 : 0) |
-                                         (cd.ct < en[2] ? 4 : 0);
                         const int ext[3] = {cd.at, cd.bt, cd.ct};
+                        const int nt[3] = {(en[0] + cd.at - 1) / cd.at, (en[1] + cd.bt - 1) / cd.bt,
+                                           (en[2] + cd.ct - 1) / cd.ct};
                         std::vector<int> seqs(ptmp.size());
                         double fl_blk = 0;
                         bool ok = true;
                         for (size_t q = 0; q < ptmp.size() && ok; ++q) {
                                 int seq[3];
                                 double fl;
-                                if (choose_seq(nops, mask, ptmp[q].eo, en, ext, &fl, seq) != 0) {
+                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, &fl, seq) != 0) {
                                         ok = false;
                                         break;
                                 }
@@ -600,6 +604,9 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 const bool placed = best_ci >= 0;
                 if (placed) {
                         const Cand cd = cand[best_ci];
+                        const int ext[3] = {cd.at, cd.bt, cd.ct};
+                        const int nt[3] = {(en[0] + cd.at - 1) / cd.at, (en[1] + cd.bt - 1) / cd.bt,
+                                           (en[2] + cd.ct - 1) / cd.ct};
                         const int pbase = (int) hp.pairs.size();
                         std::vector<double> pfl(ptmp.size());
                         for (size_t q = 0; q < ptmp.size(); ++q) {
@@ -607,7 +614,7 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                 int seq[3];
                                 for (int st = 0; st < 3; ++st) seq[st] = (best_seqs[q] >> (2 * st)) & 3;
                                 int64_t s1, s2;
-                                pfl[q] = seq_cost(seq, nops, ptmp[q].eo, en, en, &s1, &s2) *
+                                pfl[q] = seq_cost(seq, nops, ptmp[q].eo, en, ext, nt, &s1, &s2) *
                                          (ptmp[q].t1 - ptmp[q].t0);
                         }
                         flops_exec += best_fl;
