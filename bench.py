@@ -150,6 +150,7 @@ def run_engine(args, rank, world):
     sh = stream.cuda_stream
 
     peak = measure_fp64_peak(torch) if rank == 0 else None
+    tune_ms = plan.autotune(reps=2)        # the engine's autotuner picks the configuration
 
     for _ in range(args.warmup):
         plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
@@ -209,7 +210,8 @@ def run_engine(args, rank, world):
                                "one step's Heff matvec (" + os.path.basename(path) + ")",
                    **step_stats(s), "flops_per_matvec": flops,
                    "parallelism": f"replicas{world}", "l2": "flushed between iterations",
-                   "precision": "fp64"},
+                   "precision": "fp64", "kernel_config": plan.config(),
+                   "autotune_ms": tune_ms},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": traffic_from_profile(path),

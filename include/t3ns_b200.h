@@ -114,6 +114,22 @@ int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y);
 int t3ns_heff_diagonal_device(t3ns_heff *h, double *diag, void *stream);
 int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag);
 
+/* Kernel configurations of the matvec: 0 = one 512-thread CTA per SM with
+ * large shared-memory output tiles, 1 = two 256-thread CTAs per SM with small
+ * tiles.  Each has its own tiling of the plan (built on first use). */
+#define T3NS_NUM_CONFIGS 2
+int t3ns_heff_set_config(t3ns_heff *h, int config);
+int t3ns_heff_get_config(const t3ns_heff *h);
+
+/* Autotuner: times `reps` matvecs of every configuration on the plan's own
+ * stream and buffers (after one untimed run each) and makes the fastest the
+ * active one.  The choice is remembered for the plan's size bucket (powers of
+ * two of the vector length, of the largest block and of the FLOP count), and
+ * t3ns_heff_create starts every later plan of a known bucket on it; with
+ * force == 0 a plan whose bucket is known is not re-timed.  ms_out, if not
+ * NULL, receives the median time per configuration (0 when not timed). */
+int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out);
+
 /* Switch the arithmetic of subsequent matvecs (T3NS_PREC_*). */
 int t3ns_heff_set_precision(t3ns_heff *h, int precision);
 
@@ -278,6 +294,9 @@ int t3ns_precondition_device_noalloc(int64_t size, const double *result, double 
  * its work units, pair sequences and flattened terms to `path` (step-file
  * record layout), for host-side checks of the tiling and ordering. */
 int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path);
+/* The same for kernel configuration `config` (0 .. T3NS_NUM_CONFIGS-1);
+ * t3ns_heff_plan_dump writes configuration 0. */
+int t3ns_heff_plan_dump_config(const t3ns_heff_desc *desc, int config, const char *path);
 
 const char *t3ns_last_error(void);
 

@@ -1,8 +1,14 @@
 // C ABI of the engine (include/t3ns_b200.h): plan lifetime, device uploads,
 // host/device matvec entry points and error reporting.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "common.h"
 #include "heff_internal.h"
@@ -40,6 +46,37 @@ static int upload(t3ns_heff *h, T **p, const T *src, size_t n)
         return T3NS_OK;
 }
 
+// Autotuner cache: size bucket -> fastest configuration.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, int> g_tune_cache;
+
+static std::tuple<int, int, int> size_bucket(const HostPlan &hp)
+{
+        int64_t maxblk = 1;
+        for (int b = 0; b < hp.nblocks; ++b)
+                maxblk = std::max<int64_t>(maxblk, hp.block_off[b + 1] - hp.block_off[b]);
+        auto lg = [](double v) { return v > 1 ? (int) std::floor(std::log2(v)) : 0; };
+        return {lg((double) hp.size), lg((double) maxblk), lg(hp.flops_ref)};
+}
+
+// Device copy of the tiling for configuration cfg (tiled on first use).
+static int upload_tiles(t3ns_heff *h, int cfg)
+{
+        DeviceTiles &dt = h->dp.tiles[cfg];
+        if (dt.built) return T3NS_OK;
+        T3NS_TRY(tile_plan(h->hp, cfg));
+        const TilePlan &tp = h->hp.tiles[cfg];
+        T3NS_TRY(upload(h, &dt.pair_ptr, tp.pair_ptr.data(), tp.pair_ptr.size()));
+        T3NS_TRY(upload(h, &dt.pairs, tp.pairs.data(), tp.pairs.size()));
+        T3NS_TRY(upload(h, &dt.units, tp.units.data(), tp.units.size()));
+        dt.n_units = (int) tp.units.size();
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        dt.grid = std::max(1, std::min(dt.n_units, kCfgs[cfg].ctas_per_sm * sms));
+        dt.built = true;
+        return T3NS_OK;
+}
+
 static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
 {
         T3NS_CUDA_TRY(cudaGetDevice(&h->device));
@@ -66,15 +103,15 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
         T3NS_TRY(upload(h, &dp.edims, hp.edims.data(), hp.edims.size()));
         T3NS_TRY(upload(h, &dp.task_ptr, hp.task_ptr.data(), hp.task_ptr.size()));
         T3NS_TRY(upload(h, &dp.tasks, hp.tasks.data(), hp.tasks.size()));
-        T3NS_TRY(upload(h, &dp.pair_ptr, hp.pair_ptr.data(), hp.pair_ptr.size()));
-        T3NS_TRY(upload(h, &dp.pairs, hp.pairs.data(), hp.pairs.size()));
-        T3NS_TRY(upload(h, &dp.units, hp.units.data(), hp.units.size()));
-        dp.n_units = (int) hp.units.size();
+        int cfg = 0;
+        {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                auto it = g_tune_cache.find(size_bucket(hp));
+                if (it != g_tune_cache.end()) cfg = it->second;
+        }
+        T3NS_TRY(upload_tiles(h, cfg));
+        dp.active = cfg;
         T3NS_TRY(dev_alloc(h, &dp.counter, 1));
-
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-        dp.grid = std::max(1, std::min(dp.n_units, 2 * sms));
         T3NS_TRY(dev_alloc(h, &dp.err, 1));
         T3NS_CUDA_TRY(cudaMemset(dp.err, 0, sizeof(int)));
         T3NS_TRY(dev_alloc(h, &h->stage_x, (size_t) hp.size));
@@ -161,6 +198,71 @@ int t3ns_heff_set_precision(t3ns_heff *h, int precision)
         return T3NS_OK;
 }
 
+int t3ns_heff_set_config(t3ns_heff *h, int config)
+{
+        if (!h) return set_error(T3NS_E_ARG, "null plan");
+        if (config < 0 || config >= kNumCfgs) return set_error(T3NS_E_ARG, "unknown configuration");
+        T3NS_TRY(upload_tiles(h, config));
+        h->dp.active = config;
+        return T3NS_OK;
+}
+
+int t3ns_heff_get_config(const t3ns_heff *h) { return h ? h->dp.active : -1; }
+
+int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
+{
+        if (!h) return set_error(T3NS_E_ARG, "null plan");
+        if (ms_out)
+                for (int c = 0; c < kNumCfgs; ++c) ms_out[c] = 0.0;
+        const auto key = size_bucket(h->hp);
+        if (!force) {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                auto it = g_tune_cache.find(key);
+                if (it != g_tune_cache.end()) return t3ns_heff_set_config(h, it->second);
+        }
+        reps = std::max(reps, 1);
+        cudaEvent_t e0, e1;
+        T3NS_CUDA_TRY(cudaEventCreate(&e0));
+        T3NS_CUDA_TRY(cudaEventCreate(&e1));
+        int best = h->dp.active;
+        double best_ms = 0;
+        int rc = T3NS_OK;
+        for (int c = 0; c < kNumCfgs && rc == T3NS_OK; ++c) {
+                rc = t3ns_heff_set_config(h, c);
+                if (rc != T3NS_OK) break;
+                // one untimed run, then `reps` timed ones
+                rc = launch_heff_fp64(h->dp, h->stage_x, h->stage_y, h->stream, nullptr);
+                std::vector<float> t;
+                for (int r = 0; r < reps && rc == T3NS_OK; ++r) {
+                        cudaEventRecord(e0, h->stream);
+                        rc = launch_heff_fp64(h->dp, h->stage_x, h->stage_y, h->stream, nullptr);
+                        cudaEventRecord(e1, h->stream);
+                        float ms = 0;
+                        if (cudaEventSynchronize(e1) != cudaSuccess ||
+                            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+                                rc = set_error(T3NS_E_CUDA, "autotune: event timing failed");
+                        t.push_back(ms);
+                }
+                if (rc != T3NS_OK) break;
+                std::sort(t.begin(), t.end());
+                const double med = t[t.size() / 2];
+                if (ms_out) ms_out[c] = med;
+                if (c == 0 || med < best_ms) {
+                        best = c;
+                        best_ms = med;
+                }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        T3NS_TRY(rc);
+        T3NS_TRY(check_device_error(h));
+        {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tune_cache[key] = best;
+        }
+        return t3ns_heff_set_config(h, best);
+}
+
 int t3ns_heff_get_stats(const t3ns_heff *h, t3ns_heff_stats *st)
 {
         if (!h || !st) return set_error(T3NS_E_ARG, "null argument");
@@ -169,7 +271,7 @@ int t3ns_heff_get_stats(const t3ns_heff *h, t3ns_heff_stats *st)
         st->npairs = h->hp.npairs;
         st->ntasks = (int64_t) h->hp.tasks.size();
         st->flops_ref = h->hp.flops_ref;
-        st->flops_exec = h->hp.flops_exec;
+        st->flops_exec = h->hp.tiles[h->dp.active].flops_exec;
         st->bytes_alg = h->hp.bytes_alg;
         st->op_elems = h->hp.op_elems;
         st->scratch_bytes = 0;
@@ -188,8 +290,15 @@ void t3ns_heff_destroy(t3ns_heff *h)
 
 int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path)
 {
+        return t3ns_heff_plan_dump_config(desc, 0, path);
+}
+
+int t3ns_heff_plan_dump_config(const t3ns_heff_desc *desc, int config, const char *path)
+{
         HostPlan hp;
         T3NS_TRY(build_plan(desc, hp));
+        if (config < 0 || config >= kNumCfgs) return set_error(T3NS_E_ARG, "unknown configuration");
+        T3NS_TRY(tile_plan(hp, config));
         FILE *f = fopen(path, "wb");
         if (!f) return set_error(T3NS_E_ARG, std::string("cannot open ") + path);
         auto put = [&](const char *name, int dtype, int64_t n, const void *a) {
@@ -203,8 +312,9 @@ int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path)
         };
         fwrite("T3NSCAP1", 1, 8, f);
         std::vector<int> units, pairs, edims;
-        for (auto &u : hp.units) { units.insert(units.end(), {u.nb, u.b0, u.bt, u.c0, u.ct, u.a0, u.at, u.p0, u.p1, u.split}); }
-        for (auto &p : hp.pairs) { pairs.insert(pairs.end(), {p.old, p.axes, p.t0, p.t1}); }
+        const TilePlan &tp = hp.tiles[config];
+        for (auto &u : tp.units) { units.insert(units.end(), {u.nb, u.b0, u.bt, u.c0, u.ct, u.a0, u.at, u.p0, u.p1, u.split}); }
+        for (auto &p : tp.pairs) { pairs.insert(pairs.end(), {p.old, p.axes, p.t0, p.t1}); }
         for (auto &e : hp.edims) { edims.insert(edims.end(), {e.x, e.y, e.z}); }
         std::vector<int64_t> offs;
         std::vector<double> prefs;
@@ -214,11 +324,11 @@ int t3ns_heff_plan_dump(const t3ns_heff_desc *desc, const char *path)
         }
         put("plan.units", 1, (int64_t) units.size(), units.data());
         put("plan.pairs", 1, (int64_t) pairs.size(), pairs.data());
-        put("plan.pair_ptr", 1, (int64_t) hp.pair_ptr.size(), hp.pair_ptr.data());
+        put("plan.pair_ptr", 1, (int64_t) tp.pair_ptr.size(), tp.pair_ptr.data());
         put("plan.edims", 1, (int64_t) edims.size(), edims.data());
         put("plan.op_off", 2, (int64_t) offs.size(), offs.data());
         put("plan.pref", 3, (int64_t) prefs.size(), prefs.data());
-        put("plan.flops", 3, 2, std::vector<double>{hp.flops_ref, hp.flops_exec}.data());
+        put("plan.flops", 3, 2, std::vector<double>{hp.flops_ref, tp.flops_exec}.data());
         fclose(f);
         return T3NS_OK;
 }

@@ -582,6 +582,10 @@ void init_Heffdata(struct Heffdata *data, const struct rOperators *Operators,
         t3ns_heff *plan = NULL;
         if (t3ns_heff_create(&desc, precision_from_env(), &plan) != T3NS_OK)
                 die("init_Heffdata");
+        /* the first step of each size bucket times the kernel configurations */
+        const char *tune = getenv("T3NS_B200_AUTOTUNE");
+        if ((!tune || strcmp(tune, "0")) && t3ns_heff_autotune(plan, 1, 0, NULL) != T3NS_OK)
+                die("init_Heffdata (autotune)");
         plan_put(data, plan);
 
         for (int i = 0; i < (data->isdmrg ? 2 : 3); ++i)

@@ -46,14 +46,34 @@
 
 namespace t3ns {
 
-constexpr int kThreads = 256;
-constexpr int kOutCap = 2048;     // doubles: shared output tile
-constexpr int kPsiCap = 3072;     // doubles: staged old block (else read from L2)
-constexpr int kWCap = 8192;       // doubles: intermediates of a group
 constexpr int kGMax = 64;         // terms per group
 constexpr double kPairVisitCost = 4e4;   // FLOP-equivalent of one (unit, pair) visit
-constexpr size_t kSmemBytes = sizeof(double) * (kOutCap + kPsiCap + kWCap + kGMax) +
-                              sizeof(int64_t) * 3 * kGMax + 64;
+
+// Kernel configurations.  The large one (one 512-thread CTA per SM, 208 KB of
+// shared buffers) tiles fewer blocks and hides latency with 16 warps; the
+// small one (two 256-thread CTAs per SM) suits steps of many small blocks.
+// Both use all 64K registers of an SM (124 per thread at most).
+struct CfgLarge {
+        static constexpr int kThreads = 512, kMinBlocks = 1;
+        static constexpr int kOut = 8192, kPsi = 4096, kW = 14336;
+};
+struct CfgSmall {
+        static constexpr int kThreads = 256, kMinBlocks = 2;
+        static constexpr int kOut = 2048, kPsi = 3072, kW = 8192;
+};
+const KernelCfg kCfgs[kNumCfgs] = {
+        {CfgLarge::kThreads, CfgLarge::kMinBlocks, CfgLarge::kOut, CfgLarge::kPsi, CfgLarge::kW,
+         "fp64-512x1-out8192"},
+        {CfgSmall::kThreads, CfgSmall::kMinBlocks, CfgSmall::kOut, CfgSmall::kPsi, CfgSmall::kW,
+         "fp64-256x2-out2048"},
+};
+
+template <class Cfg>
+constexpr size_t smem_bytes()
+{
+        return sizeof(double) * (Cfg::kOut + Cfg::kPsi + Cfg::kW + kGMax) +
+               sizeof(int64_t) * 3 * kGMax + 64;
+}
 
 // D(8x8) += A(8x4) * B(4x8) on the FP64 tensor pipe (one warp).  Fragment
 // layout (PTX ISA, mma.m8n8k4 .f64): lane l holds A[l/4][l%4], B[l%4][l/4]
@@ -120,7 +140,7 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
 // `out` instead (which then has no term stride).  Each warp owns
 // (8*RM) x (8*RN) output tiles and runs their K loop on the FP64 tensor
 // pipe; with ACC the group reduction stays inside the warp's accumulators.
-template <bool ACC, int RM, int RN>
+template <bool ACC, int RM, int RN, int NW>
 __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, int ldop, int G,
                                                 const int64_t *opoff,
                                                 const double *__restrict__ ops, const double *in,
@@ -145,7 +165,7 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
         const int items = (ACC ? 1 : G) * nc * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int lr = lane >> 2, lc = lane & 3;
-        for (int it = warp; it < items; it += kThreads / 32) {
+        for (int it = warp; it < items; it += NW) {
                 const int tile = it % tiles;
                 const int gc = it / tiles;
                 const int tm = tile % mt, tn = tile / mt;
@@ -187,7 +207,7 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
 
 // Warp-tile shape per stage: 8x32 when M is small, 32x8 when N is small,
 // else 16x16.
-template <bool ACC>
+template <bool ACC, int NW>
 __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
                                               const int64_t *opoff,
                                               const double *__restrict__ ops, const double *in,
@@ -197,14 +217,15 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
         const int M = ax == 0 ? rows : ax == 1 ? w[0] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
         if (M <= 8)
-                grouped_stage_t<ACC, 1, 4>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+                grouped_stage_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
         else if (N <= 8)
-                grouped_stage_t<ACC, 4, 1>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+                grouped_stage_t<ACC, 4, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
         else
-                grouped_stage_t<ACC, 2, 2>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+                grouped_stage_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::kThreads, Cfg::kMinBlocks)
 heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                  const double *__restrict__ ops, const int64_t *__restrict__ blk_off,
                  const int4 *__restrict__ edims, const HeffUnit *__restrict__ units, int n_units,
@@ -213,9 +234,10 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
 {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         double *OUT = reinterpret_cast<double *>(smem_raw);
-        double *PSI = OUT + kOutCap;
-        double *W = PSI + kPsiCap;
-        double *PREF = W + kWCap;
+        constexpr int kThreads = Cfg::kThreads, NW = Cfg::kThreads / 32;
+        double *PSI = OUT + Cfg::kOut;
+        double *W = PSI + Cfg::kPsi;
+        double *PREF = W + Cfg::kW;
         int64_t *OPOFF = reinterpret_cast<int64_t *>(PREF + kGMax);   // [3][kGMax]
         int *UNIT = reinterpret_cast<int *>(OPOFF + 3 * kGMax);
         const int tid = threadIdx.x;
@@ -250,17 +272,17 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                         const int s0 = w0[0] * w0[1] * w0[2];
                         const int s1 = w1[0] * w1[1] * w1[2];
                         const int s2 = nst == 3 ? w2[0] * w2[1] * w2[2] : 0;
-                        if (s1 + s2 > kWCap) {
+                        if (s1 + s2 > Cfg::kW) {
                                 if (tid == 0) atomicExch(err, 3);
                                 return;
                         }
                         const double *xin = x + blk_off[pr.old];
                         const double *in0 = xin;
-                        if (s0 <= kPsiCap) {
+                        if (s0 <= Cfg::kPsi) {
                                 for (int e = tid; e < s0; e += kThreads) PSI[e] = xin[e];
                                 in0 = PSI;
                         }
-                        const int G = min(kGMax, kWCap / (s1 + s2));
+                        const int G = min(kGMax, Cfg::kW / (s1 + s2));
                         double *W1 = W, *W2 = W + G * s1;
                         const int nterm = pr.t1 - pr.t0;
                         for (int t0 = 0; t0 < nterm; t0 += G) {
@@ -273,20 +295,20 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                                 }
                                 __syncthreads();
                                 if (nst == 3) {
-                                        grouped_stage<false>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
+                                        grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
                                                              ops, in0, 0, W1, s1, nullptr);
                                         __syncthreads();
-                                        grouped_stage<false>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
+                                        grouped_stage<false, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
                                                              OPOFF + kGMax, ops, W1, s1, W2, s2, PREF);
                                         __syncthreads();
-                                        grouped_stage<true>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
+                                        grouped_stage<true, NW>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
                                                             OPOFF + 2 * kGMax, ops, W2, s2, OUT, 0,
                                                             nullptr);
                                 } else {
-                                        grouped_stage<false>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
+                                        grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
                                                              ops, in0, 0, W1, s1, PREF);
                                         __syncthreads();
-                                        grouped_stage<true>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
+                                        grouped_stage<true, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
                                                             OPOFF + kGMax, ops, W1, s1, OUT, 0,
                                                             nullptr);
                                 }
@@ -380,7 +402,7 @@ static double seq_cost(const int *seq, int nst, const int *o, const int *n, cons
 // Cheapest contraction sequence for a pair on a tiling (ext, nt) among those
 // whose intermediates fit the shared buffer.  Returns -1 if none fits.
 static int choose_seq(int nst, const int *o, const int *n, const int *ext, const int *nt,
-                      double *fl_out, int seq_out[3])
+                      int w_cap, double *fl_out, int seq_out[3])
 {
         static const int perms3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
                                          {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
@@ -392,7 +414,7 @@ static int choose_seq(int nst, const int *o, const int *n, const int *ext, const
                 const int *seq = nst == 3 ? perms3[q] : perms2[q];
                 int64_t s1 = 0, s2 = 0;
                 const double fl = seq_cost(seq, nst, o, n, ext, nt, &s1, &s2);
-                if (s1 + s2 > kWCap) continue;
+                if (s1 + s2 > w_cap) continue;
                 if (best < 0 || fl < bfl) { best = q; bfl = fl; }
         }
         if (best < 0) return -1;
@@ -447,14 +469,10 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
 
         // terms, grouped by pair, pairs by new block
         hp.task_ptr.assign(d->nblocks + 1, 0);
-        hp.pair_ptr.assign(d->nblocks + 1, 0);
         hp.tasks.clear();
-        hp.pairs.clear();
-        hp.units.clear();
-        double flops_ref = 0, flops_exec = 0;
+        for (auto &tp : hp.tiles) tp = TilePlan();
+        double flops_ref = 0;
         int64_t npairs = 0;
-        std::vector<double> unit_work;
-        struct PairTmp { int ob; int t0, t1; int eo[3]; };
         std::vector<std::vector<PairTmp>> blocks_pairs(d->nblocks);
         for (int nb = 0; nb < d->nblocks; ++nb) {
                 hp.task_ptr[nb] = (int) hp.tasks.size();
@@ -524,12 +542,52 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 blocks_pairs[nb] = std::move(ptmp);
         }
         hp.task_ptr[d->nblocks] = (int) hp.tasks.size();
+        if (hp.tasks.size() > (size_t) INT32_MAX)
+                return set_error(T3NS_E_LIMIT, "more than 2^31 tasks");
+        hp.blocks_pairs = std::move(blocks_pairs);
+        hp.npairs = npairs;
+        hp.flops_ref = flops_ref;
+
+        // algorithmic bytes: vectors in/out + each referenced operator block once
+        {
+                std::vector<std::pair<int64_t, int64_t>> blocks;
+                blocks.reserve(hp.tasks.size() * nops);
+                for (int nb = 0; nb < d->nblocks; ++nb)
+                        for (int t = hp.task_ptr[nb]; t < hp.task_ptr[nb + 1]; ++t) {
+                                const HeffTask &tk = hp.tasks[t];
+                                const int4 eo = hp.edims[tk.old], en = hp.edims[nb];
+                                const int o3[3] = {eo.x, eo.y, eo.z}, n3[3] = {en.x, en.y, en.z};
+                                for (int j = 0; j < nops; ++j)
+                                        blocks.push_back({tk.op_off[j], (int64_t) o3[j] * n3[j]});
+                        }
+                std::sort(blocks.begin(), blocks.end());
+                blocks.erase(std::unique(blocks.begin(), blocks.end()), blocks.end());
+                double opbytes = 0;
+                for (auto &b : blocks) opbytes += 8.0 * b.second;
+                hp.bytes_alg = 16.0 * hp.size + opbytes;
+        }
+        return tile_plan(hp, 0);
+}
+
+
+int tile_plan(HostPlan &hp, int cfg)
+{
+        if (cfg < 0 || cfg >= kNumCfgs) return set_error(T3NS_E_ARG, "unknown kernel configuration");
+        TilePlan &tp = hp.tiles[cfg];
+        if (tp.built) return T3NS_OK;
+        const KernelCfg &kc = kCfgs[cfg];
+        const int nops = hp.isdmrg ? 2 : 3;
+        tp.pair_ptr.assign(hp.nblocks + 1, 0);
+        tp.pairs.clear();
+        tp.units.clear();
+        double flops_exec = 0;
+        std::vector<double> unit_work;
         // a unit should not carry more than a small share of the work, so the
         // heaviest-first schedule ends evenly across the CTAs
-        const double unit_cap = std::max(flops_ref / (148.0 * 2 * 8), 1e6);
-        for (int nb = 0; nb < d->nblocks; ++nb) {
-                hp.pair_ptr[nb] = (int) hp.pairs.size();
-                auto &ptmp = blocks_pairs[nb];
+        const double unit_cap = std::max(hp.flops_ref / (148.0 * kc.ctas_per_sm * 8), 1e6);
+        for (int nb = 0; nb < hp.nblocks; ++nb) {
+                tp.pair_ptr[nb] = (int) tp.pairs.size();
+                auto &ptmp = hp.blocks_pairs[nb];
                 if (ptmp.empty()) continue;
                 const int4 en4 = hp.edims[nb];
                 const int en[3] = {en4.x, en4.y, en4.z};
@@ -540,11 +598,11 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 struct Cand { int at, bt, ct; };
                 std::vector<Cand> cand;
                 const int64_t sn = (int64_t) en[0] * en[1] * en[2];
-                if (sn <= kOutCap) cand.push_back({en[0], en[1], en[2]});
+                if (sn <= kc.out_cap) cand.push_back({en[0], en[1], en[2]});
                 for (int ax = 0; ax < 3; ++ax) {
                         const int64_t rest = sn / std::max(en[ax], 1);
-                        if (rest == 0 || rest > kOutCap) continue;
-                        for (int t = (int) std::min<int64_t>(en[ax], kOutCap / rest); t >= 1; t /= 2) {
+                        if (rest == 0 || rest > kc.out_cap) continue;
+                        for (int t = (int) std::min<int64_t>(en[ax], kc.out_cap / rest); t >= 1; t /= 2) {
                                 if (t == en[ax]) continue;
                                 Cand c{en[0], en[1], en[2]};
                                 (ax == 0 ? c.at : ax == 1 ? c.bt : c.ct) = t;
@@ -555,8 +613,8 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         // tile axis p1 with t, axis p2 with 1
                         const int p1 = pair == 2 ? 0 : pair + 1, p2 = pair == 2 ? 1 : (pair == 0 ? 2 : 0);
                         const int other = 3 - p1 - p2;
-                        if (en[other] > kOutCap || en[p2] <= 1) continue;
-                        for (int t = std::min(en[p1], kOutCap / std::max(en[other], 1)); t >= 1; t /= 2) {
+                        if (en[other] > kc.out_cap || en[p2] <= 1) continue;
+                        for (int t = std::min(en[p1], kc.out_cap / std::max(en[other], 1)); t >= 1; t /= 2) {
                                 Cand c{en[0], en[1], en[2]};
                                 (p1 == 0 ? c.at : p1 == 1 ? c.bt : c.ct) = t;
                                 (p2 == 0 ? c.at : p2 == 1 ? c.bt : c.ct) = 1;
@@ -577,7 +635,7 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         for (size_t q = 0; q < ptmp.size() && ok; ++q) {
                                 int seq[3];
                                 double fl;
-                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, &fl, seq) != 0) {
+                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, kc.w_cap, &fl, seq) != 0) {
                                         ok = false;
                                         break;
                                 }
@@ -607,10 +665,10 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         const int ext[3] = {cd.at, cd.bt, cd.ct};
                         const int nt[3] = {(en[0] + cd.at - 1) / cd.at, (en[1] + cd.bt - 1) / cd.bt,
                                            (en[2] + cd.ct - 1) / cd.ct};
-                        const int pbase = (int) hp.pairs.size();
+                        const int pbase = (int) tp.pairs.size();
                         std::vector<double> pfl(ptmp.size());
                         for (size_t q = 0; q < ptmp.size(); ++q) {
-                                hp.pairs.push_back({ptmp[q].ob, best_seqs[q], ptmp[q].t0, ptmp[q].t1});
+                                tp.pairs.push_back({ptmp[q].ob, best_seqs[q], ptmp[q].t0, ptmp[q].t1});
                                 int seq[3];
                                 for (int st = 0; st < 3; ++st) seq[st] = (best_seqs[q] >> (2 * st)) & 3;
                                 int64_t s1, s2;
@@ -650,7 +708,7 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                                         v.p0 = pbase + (int) q;
                                                         v.p1 = pbase + (int) q1;
                                                         v.split = split ? 1 : 0;
-                                                        hp.units.push_back(v);
+                                                        tp.units.push_back(v);
                                                         unit_work.push_back(w + 1e4 * (q1 - q));
                                                         q = q1;
                                                 }
@@ -660,64 +718,53 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         return set_error(T3NS_E_LIMIT, "no tiling of output block " + std::to_string(nb) +
                                                                " fits the shared-memory buffers");
         }
-        hp.pair_ptr[d->nblocks] = (int) hp.pairs.size();
-        if (hp.tasks.size() > (size_t) INT32_MAX)
-                return set_error(T3NS_E_LIMIT, "more than 2^31 tasks");
-        hp.npairs = npairs;
-        hp.flops_ref = flops_ref;
-        hp.flops_exec = flops_exec;
+        tp.pair_ptr[hp.nblocks] = (int) tp.pairs.size();
+        tp.flops_exec = flops_exec;
 
         // heaviest units first
-        std::vector<int> idx(hp.units.size());
+        std::vector<int> idx(tp.units.size());
         std::iota(idx.begin(), idx.end(), 0);
         std::stable_sort(idx.begin(), idx.end(),
                          [&](int a, int b) { return unit_work[a] > unit_work[b]; });
-        std::vector<HeffUnit> sorted(hp.units.size());
-        for (size_t i = 0; i < idx.size(); ++i) sorted[i] = hp.units[idx[i]];
-        hp.units.swap(sorted);
+        std::vector<HeffUnit> sorted(tp.units.size());
+        for (size_t i = 0; i < idx.size(); ++i) sorted[i] = tp.units[idx[i]];
+        tp.units.swap(sorted);
 
-        // algorithmic bytes: vectors in/out + each referenced operator block once
-        {
-                std::vector<std::pair<int64_t, int64_t>> blocks;
-                blocks.reserve(hp.tasks.size() * nops);
-                for (int nb = 0; nb < d->nblocks; ++nb)
-                        for (int t = hp.task_ptr[nb]; t < hp.task_ptr[nb + 1]; ++t) {
-                                const HeffTask &tk = hp.tasks[t];
-                                const int4 eo = hp.edims[tk.old], en = hp.edims[nb];
-                                const int o3[3] = {eo.x, eo.y, eo.z}, n3[3] = {en.x, en.y, en.z};
-                                for (int j = 0; j < nops; ++j)
-                                        blocks.push_back({tk.op_off[j], (int64_t) o3[j] * n3[j]});
-                        }
-                std::sort(blocks.begin(), blocks.end());
-                blocks.erase(std::unique(blocks.begin(), blocks.end()), blocks.end());
-                double opbytes = 0;
-                for (auto &b : blocks) opbytes += 8.0 * b.second;
-                hp.bytes_alg = 16.0 * hp.size + opbytes;
+        tp.built = true;
+        return T3NS_OK;
+}
+
+template <class Cfg>
+static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const double *x, double *y,
+                      cudaStream_t s)
+{
+        static bool attr_set = false;   // per configuration (one instantiation each)
+        if (!attr_set) {
+                T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_fp64_kernel<Cfg>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int) smem_bytes<Cfg>()));
+                attr_set = true;
         }
+        heff_fp64_kernel<Cfg><<<dt.grid, Cfg::kThreads, smem_bytes<Cfg>(), s>>>(
+                x, y, dp.ops, dp.blk_off, dp.edims, dt.units, dt.n_units, dt.pair_ptr, dt.pairs,
+                dp.tasks, dp.counter, dp.err);
+        T3NS_CUDA_TRY(cudaGetLastError());
         return T3NS_OK;
 }
 
 int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStream_t s,
                      int *launches)
 {
+        const DeviceTiles &dt = dp.tiles[dp.active];
+        if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
         T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
-        if (dp.n_units > 0) {
-                static bool attr_set = false;
-                if (!attr_set) {
-                        T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_fp64_kernel,
-                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                           (int) kSmemBytes));
-                        attr_set = true;
-                }
-                T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
-                heff_fp64_kernel<<<dp.grid, kThreads, kSmemBytes, s>>>(
-                        x, y, dp.ops, dp.blk_off, dp.edims, dp.units, dp.n_units, dp.pair_ptr,
-                        dp.pairs, dp.tasks, dp.counter, dp.err);
-                T3NS_CUDA_TRY(cudaGetLastError());
-                if (launches) *launches = 1;
-        } else if (launches) {
-                *launches = 0;
-        }
+        if (launches) *launches = 0;
+        if (dt.n_units == 0) return T3NS_OK;
+        T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
+        static_assert(kNumCfgs == 2, "one launch branch per configuration");
+        T3NS_TRY(dp.active == 0 ? launch_cfg<CfgLarge>(dp, dt, x, y, s)
+                                : launch_cfg<CfgSmall>(dp, dt, x, y, s));
+        if (launches) *launches = 1;
         return T3NS_OK;
 }
 

@@ -41,6 +41,35 @@ struct __align__(16) HeffUnit {
         int pad[2];
 };
 
+// Kernel configurations (launch shape and shared-memory buffers, in
+// elements of the compute type); a plan is tiled for one of them.
+struct KernelCfg {
+        int threads;       // per CTA
+        int ctas_per_sm;   // resident CTAs per SM the launch is sized for
+        int out_cap;       // output tile
+        int psi_cap;       // staged old block
+        int w_cap;         // intermediates of a group of terms
+        const char *name;
+};
+constexpr int kNumCfgs = 2;
+extern const KernelCfg kCfgs[kNumCfgs];
+
+// One (new, old) pair before tiling: its terms and the old block's dims.
+struct PairTmp {
+        int ob;
+        int t0, t1;
+        int eo[3];
+};
+
+// The pairs and work units of a plan tiled for one kernel configuration.
+struct TilePlan {
+        bool built = false;
+        std::vector<int> pair_ptr;                // [nblocks + 1] into pairs
+        std::vector<HeffPair> pairs;
+        std::vector<HeffUnit> units;              // heaviest first
+        double flops_exec = 0;
+};
+
 struct HostPlan {
         int isdmrg = 0;
         int map[3] = {0, 1, 2};
@@ -52,12 +81,20 @@ struct HostPlan {
         int64_t op_elems = 0;
         std::vector<int> task_ptr;
         std::vector<HeffTask> tasks;
-        std::vector<int> pair_ptr;                // [nblocks + 1] into pairs
-        std::vector<HeffPair> pairs;
-        std::vector<int> work_order;
-        std::vector<HeffUnit> units;              // heaviest first
+        std::vector<std::vector<PairTmp>> blocks_pairs;   // per new block
+        TilePlan tiles[kNumCfgs];
         int64_t npairs = 0;
-        double flops_ref = 0, flops_exec = 0, bytes_alg = 0;
+        double flops_ref = 0, bytes_alg = 0;
+};
+
+// Device copy of one tiling.
+struct DeviceTiles {
+        bool built = false;
+        int *pair_ptr = nullptr;
+        HeffPair *pairs = nullptr;
+        HeffUnit *units = nullptr;
+        int n_units = 0;
+        int grid = 0;
 };
 
 struct DevicePlan {
@@ -66,20 +103,19 @@ struct DevicePlan {
         double *ops = nullptr;
         int64_t *blk_off = nullptr;
         int4 *edims = nullptr;
-        int *work_order = nullptr;
-        int n_active = 0;
         int *task_ptr = nullptr;
         HeffTask *tasks = nullptr;
-        int *pair_ptr = nullptr;
-        HeffPair *pairs = nullptr;
-        HeffUnit *units = nullptr;
-        int n_units = 0;
+        DeviceTiles tiles[kNumCfgs];
+        int active = 0;                           // configuration the matvec runs
         int *counter = nullptr;                   // dynamic unit scheduler
-        int grid = 0;
         int *err = nullptr;
 };
 
+// Shared part of the plan (terms, block tables) and the tiling for
+// configuration 0.
 int build_plan(const t3ns_heff_desc *d, HostPlan &hp);
+// Tiling of hp for configuration cfg (hp.tiles[cfg]).
+int tile_plan(HostPlan &hp, int cfg);
 int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStream_t s,
                      int *launches);
 int launch_heff_diag(const DevicePlan &dp, double *diag, cudaStream_t s);

