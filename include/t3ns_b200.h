@@ -147,11 +147,16 @@ typedef struct {
         double d_energy;         /* last energy change                         */
         double residual;         /* final residual norm                        */
         double seconds;          /* wall time of the solve                     */
+        int fp64_iterations;     /* of those, iterations with an FP64 matvec   */
 } t3ns_davidson_info;
 
 /* Davidson for the lowest eigenpair, device resident (reference
  * src/davidson.c:259-328: same subspace bound, deflation, Olsen-corrected
- * diagonal preconditioner with cutoff 1e-12, and stopping rule).  `result`
+ * diagonal preconditioner with cutoff 1e-12, and stopping rule).  With the
+ * plan in T3NS_PREC_3XTF32 the solve runs its iterations on the
+ * split-precision matvec until the residual reaches tol or stops improving,
+ * then continues from that vector with FP64 matvecs (defect correction) until
+ * the FP64 residual reaches tol, so energy and residual are FP64 quantities.  `result`
  * holds the initial guess and receives the normalised eigenvector; `energy`
  * receives the Ritz value.  Returns 0 when converged, 1 when max_its was
  * reached, T3NS_E* on failure.  `info` may be NULL. */

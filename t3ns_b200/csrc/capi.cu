@@ -48,15 +48,15 @@ static int upload(t3ns_heff *h, T **p, const T *src, size_t n)
 
 // Autotuner cache: size bucket -> fastest configuration.
 static std::mutex g_tune_mu;
-static std::map<std::tuple<int, int, int>, int> g_tune_cache;
+static std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 
-static std::tuple<int, int, int> size_bucket(const HostPlan &hp)
+static std::tuple<int, int, int, int> size_bucket(const HostPlan &hp, int precision)
 {
         int64_t maxblk = 1;
         for (int b = 0; b < hp.nblocks; ++b)
                 maxblk = std::max<int64_t>(maxblk, hp.block_off[b + 1] - hp.block_off[b]);
         auto lg = [](double v) { return v > 1 ? (int) std::floor(std::log2(v)) : 0; };
-        return {lg((double) hp.size), lg((double) maxblk), lg(hp.flops_ref)};
+        return {lg((double) hp.size), lg((double) maxblk), lg(hp.flops_ref), precision};
 }
 
 // Device copy of the tiling for configuration cfg (tiled on first use).
@@ -77,13 +77,31 @@ static int upload_tiles(t3ns_heff *h, int cfg)
         return T3NS_OK;
 }
 
+// FP32 operator copy and input staging of the split-precision matvec.
+static int setup_precision(t3ns_heff *h, int precision)
+{
+        if (precision == T3NS_PREC_BF16X3)
+                return set_error(T3NS_E_ARG, "BF16x3 matvec is not built in this library "
+                                             "(use T3NS_PREC_3XTF32)");
+        if (precision != T3NS_PREC_FP64 && precision != T3NS_PREC_3XTF32)
+                return set_error(T3NS_E_ARG, "unknown precision");
+        DevicePlan &dp = h->dp;
+        if (precision == T3NS_PREC_3XTF32 && !dp.ops32) {
+                T3NS_TRY(dev_alloc(h, &dp.ops32, (size_t) h->hp.op_elems));
+                T3NS_TRY(dev_alloc(h, &dp.x32, (size_t) h->hp.size));
+                T3NS_TRY(convert_to_f32(dp.ops, dp.ops32, h->hp.op_elems, h->stream));
+                T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        }
+        h->precision = precision;
+        return T3NS_OK;
+}
+
 static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
 {
         T3NS_CUDA_TRY(cudaGetDevice(&h->device));
         T3NS_TRY(build_plan(desc, h->hp));
         HostPlan &hp = h->hp;
         DevicePlan &dp = h->dp;
-        h->precision = precision;
         dp.nblocks = hp.nblocks;
         dp.size = hp.size;
 
@@ -106,7 +124,7 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
         int cfg = 0;
         {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
-                auto it = g_tune_cache.find(size_bucket(hp));
+                auto it = g_tune_cache.find(size_bucket(hp, precision));
                 if (it != g_tune_cache.end()) cfg = it->second;
         }
         T3NS_TRY(upload_tiles(h, cfg));
@@ -117,7 +135,7 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
         T3NS_TRY(dev_alloc(h, &h->stage_x, (size_t) hp.size));
         T3NS_TRY(dev_alloc(h, &h->stage_y, (size_t) hp.size));
         T3NS_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-        return T3NS_OK;
+        return setup_precision(h, precision);
 }
 
 static int check_device_error(t3ns_heff *h)
@@ -159,7 +177,7 @@ int t3ns_heff_create(const t3ns_heff_desc *desc, int precision, t3ns_heff **out)
 int t3ns_heff_matvec_device(t3ns_heff *h, const double *x, double *y, void *stream)
 {
         if (!h || !x || !y) return set_error(T3NS_E_ARG, "null argument");
-        return launch_heff_fp64(h->dp, x, y, (cudaStream_t) stream, &h->last_launches);
+        return launch_heff(h->dp, h->precision, x, y, (cudaStream_t) stream, &h->last_launches);
 }
 
 int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y)
@@ -167,7 +185,8 @@ int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y)
         if (!h || !x || !y) return set_error(T3NS_E_ARG, "null argument");
         const size_t bytes = sizeof(double) * h->hp.size;
         T3NS_CUDA_TRY(cudaMemcpyAsync(h->stage_x, x, bytes, cudaMemcpyHostToDevice, h->stream));
-        T3NS_TRY(launch_heff_fp64(h->dp, h->stage_x, h->stage_y, h->stream, &h->last_launches));
+        T3NS_TRY(launch_heff(h->dp, h->precision, h->stage_x, h->stage_y, h->stream,
+                             &h->last_launches));
         T3NS_CUDA_TRY(cudaMemcpyAsync(y, h->stage_y, bytes, cudaMemcpyDeviceToHost, h->stream));
         T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
         return check_device_error(h);
@@ -192,10 +211,7 @@ int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag)
 int t3ns_heff_set_precision(t3ns_heff *h, int precision)
 {
         if (!h) return set_error(T3NS_E_ARG, "null plan");
-        if (precision != T3NS_PREC_FP64)
-                return set_error(T3NS_E_ARG, "split-precision matvec is not built in this library");
-        h->precision = precision;
-        return T3NS_OK;
+        return setup_precision(h, precision);
 }
 
 int t3ns_heff_set_config(t3ns_heff *h, int config)
@@ -214,7 +230,7 @@ int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
         if (!h) return set_error(T3NS_E_ARG, "null plan");
         if (ms_out)
                 for (int c = 0; c < kNumCfgs; ++c) ms_out[c] = 0.0;
-        const auto key = size_bucket(h->hp);
+        const auto key = size_bucket(h->hp, h->precision);
         if (!force) {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 auto it = g_tune_cache.find(key);
@@ -231,11 +247,12 @@ int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
                 rc = t3ns_heff_set_config(h, c);
                 if (rc != T3NS_OK) break;
                 // one untimed run, then `reps` timed ones
-                rc = launch_heff_fp64(h->dp, h->stage_x, h->stage_y, h->stream, nullptr);
+                rc = launch_heff(h->dp, h->precision, h->stage_x, h->stage_y, h->stream, nullptr);
                 std::vector<float> t;
                 for (int r = 0; r < reps && rc == T3NS_OK; ++r) {
                         cudaEventRecord(e0, h->stream);
-                        rc = launch_heff_fp64(h->dp, h->stage_x, h->stage_y, h->stream, nullptr);
+                        rc = launch_heff(h->dp, h->precision, h->stage_x, h->stage_y, h->stream,
+                                         nullptr);
                         cudaEventRecord(e1, h->stream);
                         float ms = 0;
                         if (cudaEventSynchronize(e1) != cudaSuccess ||

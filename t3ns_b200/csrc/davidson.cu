@@ -408,9 +408,12 @@ static int alloc_basis(DavidsonBuffers &b, int64_t n, int max_vecs)
 // y = H x on device vectors, enqueued on the given stream
 using DevMatvec = std::function<int(const double *, double *, cudaStream_t)>;
 
+// stall > 0: also stop (returning 2) once the residual has not fallen below
+// 0.9 of its best value for `stall` iterations (the split-precision phase,
+// whose residual levels off at the matvec's rounding).
 static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, double *energy,
                          int max_vecs, int keep, double tol, int max_its, const double *d_diag,
-                         t3ns_davidson_info *info, cudaStream_t s)
+                         t3ns_davidson_info *info, cudaStream_t s, int stall = 0)
 {
         const auto t_start = std::chrono::steady_clock::now();
         if (max_vecs > kMaxVecs || keep > 4 || keep < 1 || keep >= max_vecs || max_vecs < 3)
@@ -433,8 +436,9 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
         T3NS_CUDA_TRY(cudaMemcpyAsync(b.t, d_result, sizeof(double) * n,
                                       cudaMemcpyDeviceToDevice, s));
         const int G = kRedBlocks, T = kRedThreads;
-        int m = 0, its = 0;
-        double res = tol * 10, e_old = 0, d_e = tol * 10;
+        int m = 0, its = 0, since_best = 0;
+        bool stalled = false;
+        double res = tol * 10, e_old = 0, d_e = tol * 10, best_res = 0;
         *energy = 0;
 
         auto column_of_S = [&](int col) -> int {
@@ -451,7 +455,7 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                 return T3NS_OK;
         };
 
-        while (res > tol && its < max_its) {
+        while (res > tol && its < max_its && !stalled) {
                 double *vm = b.V + (int64_t) m * n;
                 if (m > 0) {
                         for (int pass = 0; pass < 2; ++pass) {
@@ -494,6 +498,12 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                 memcpy(&st, b.host_scal + 4, sizeof(int));
                 if (st != 0) return set_error(T3NS_E_EIG, "davidson: subspace eigensolver did not converge");
                 res = sqrt(b.host_scal[0]);
+                if (its == 0 || res < 0.9 * best_res) {
+                        best_res = res;
+                        since_best = 0;
+                } else if (stall > 0 && ++since_best >= stall) {
+                        stalled = true;
+                }
                 const double theta = b.host_scal[3];
                 d_e = e_old - theta;
                 e_old = theta;
@@ -510,20 +520,41 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                 info->residual = res;
                 info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() -
                                                               t_start).count();
+                info->fp64_iterations = its;
         }
-        return its >= max_its ? 1 : 0;
+        if (res <= tol) return 0;
+        return stalled ? 2 : 1;
 }
 
 int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
                  int keep, double tol, int max_its, const double *d_diag,
                  t3ns_davidson_info *info, cudaStream_t s)
 {
-        DevMatvec mv = [h](const double *x, double *y, cudaStream_t st) {
-                int launches = 0;
-                return launch_heff_fp64(h->dp, x, y, st, &launches);
+        auto matvec_in = [h](int precision) {
+                return DevMatvec([h, precision](const double *x, double *y, cudaStream_t st) {
+                        int launches = 0;
+                        return launch_heff(h->dp, precision, x, y, st, &launches);
+                });
         };
-        return davidson_core(h->hp.size, mv, d_result, energy, max_vecs, keep, tol, max_its,
-                             d_diag, info, s);
+        if (h->precision == T3NS_PREC_FP64)
+                return davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy,
+                                     max_vecs, keep, tol, max_its, d_diag, info, s);
+        // split-precision iterations, then FP64 defect correction from their vector
+        t3ns_davidson_info i1{}, i2{};
+        const auto t0 = std::chrono::steady_clock::now();
+        int rc = davidson_core(h->hp.size, matvec_in(h->precision), d_result, energy, max_vecs,
+                               keep, tol, max_its, d_diag, &i1, s, /*stall=*/4);
+        if (rc < 0) return rc;
+        rc = davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy, max_vecs,
+                           keep, tol, std::max(max_its - i1.iterations, 2), d_diag, &i2, s);
+        if (rc < 0) return rc;
+        if (info) {
+                *info = i2;
+                info->iterations = i1.iterations + i2.iterations;
+                info->fp64_iterations = i2.iterations;
+                info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        return rc == 0 ? 0 : 1;
 }
 
 }  // namespace t3ns

@@ -68,12 +68,6 @@ const KernelCfg kCfgs[kNumCfgs] = {
          "fp64-256x2-out2048"},
 };
 
-template <class Cfg>
-constexpr size_t smem_bytes()
-{
-        return sizeof(double) * (Cfg::kOut + Cfg::kPsi + Cfg::kW + kGMax) +
-               sizeof(int64_t) * 3 * kGMax + 64;
-}
 
 // D(8x8) += A(8x4) * B(4x8) on the FP64 tensor pipe (one warp).  Fragment
 // layout (PTX ISA, mma.m8n8k4 .f64): lane l holds A[l/4][l%4], B[l%4][l/4]
@@ -224,20 +218,208 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                 grouped_stage_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
 }
 
-template <class Cfg>
+// ---------------------------------------------------------------------------
+// Split-precision stages: FP32 data, products on the TF32 tensor pipe
+// (mma.m16n8k8) as 3xTF32 -- x = hi + lo with hi = tf32(x), lo = tf32(x - hi),
+// x*y ~ lo_x*hi_y + hi_x*lo_y + hi_x*hi_y (the lo*lo term, ~2^-22 relative,
+// is dropped) -- with FP32 accumulation.
+
+__device__ __forceinline__ uint32_t to_tf32(float x)
+{
+        uint32_t r;
+        asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+        return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo)
+{
+        hi = to_tf32(x);
+        lo = to_tf32(x - __uint_as_float(hi));
+}
+
+// D(16x8) += A(16x8) * B(8x8).  Fragments (PTX ISA, mma.m16n8k8 .tf32), with
+// g = lane/4, t = lane%4: a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]},
+// b = {B[t][g], B[t+4][g]}, d = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}.
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
+{
+        asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, "
+                     "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                     : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                     : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Warp tile of (16*RM) x (8*RN) outputs, A(m,k) = Ab[m*am + k*ak],
+// B(k,n) = Bb[k*bk + n*bn]; loop bounds warp-uniform, lanes outside M, N or K
+// load zeros.
+template <int RM, int RN>
+__device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const float *Ab, int am,
+                                                 int ak, const float *Bb, int bk, int bn, int K,
+                                                 int M, int N, int m0, int n0, int g, int t)
+{
+        for (int k0 = 0; k0 < K; k0 += 8) {
+                const int kk[2] = {k0 + t, k0 + t + 4};
+                uint32_t ah[RM][4], al[RM][4], bh[RN][2], bl[RN][2];
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int c = 0; c < 2; ++c)
+#pragma unroll
+                                for (int r = 0; r < 2; ++r) {
+                                        const int m = m0 + 16 * i + 8 * r + g;
+                                        const float v = (m < M && kk[c] < K) ? Ab[m * am + kk[c] * ak] : 0.f;
+                                        split_tf32(v, ah[i][r + 2 * c], al[i][r + 2 * c]);
+                                }
+#pragma unroll
+                for (int j = 0; j < RN; ++j) {
+                        const int n = n0 + 8 * j + g;
+#pragma unroll
+                        for (int c = 0; c < 2; ++c) {
+                                const float v = (n < N && kk[c] < K) ? Bb[kk[c] * bk + n * bn] : 0.f;
+                                split_tf32(v, bh[j][c], bl[j][c]);
+                        }
+                }
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) {
+                                mma_tf32(d[i][j], al[i], bh[j]);
+                                mma_tf32(d[i][j], ah[i], bl[j]);
+                                mma_tf32(d[i][j], ah[i], bh[j]);
+                        }
+        }
+}
+
+// The grouped stage of the FP64 path for FP32 data.  The GEMM is taken in the
+// orientation that puts the larger of M and N on the tile's 16-row side.
+template <bool ACC, int RM, int RN, int NW>
+__device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int rows, int ldop,
+                                                    int G, const int64_t *opoff,
+                                                    const float *__restrict__ ops,
+                                                    const float *in, int in_gs, float *out,
+                                                    int out_gs, const float *scale, bool swap)
+{
+        int M, N, K, nc, ak, bk, bn, cn, a_cs, c_cs;
+        if (ax == 0) {
+                M = rows; N = w[1] * w[2]; K = w[0]; nc = 1;
+                ak = ldop; bk = 1; bn = K; cn = rows; a_cs = 0; c_cs = 0;
+        } else if (ax == 1) {
+                M = w[0]; N = rows; K = w[1]; nc = w[2];
+                ak = w[0]; bk = ldop; bn = 1; cn = w[0];
+                a_cs = w[0] * w[1]; c_cs = w[0] * rows;
+        } else {
+                M = w[0] * w[1]; N = rows; K = w[2]; nc = 1;
+                ak = M; bk = ldop; bn = 1; cn = M; a_cs = 0; c_cs = 0;
+        }
+        // tile orientation: (M', N') with A'(m',k) and B'(k,n'), C'(m',n') = C[m'*cm + n'*cnn]
+        const int Mt = swap ? N : M, Nt = swap ? M : N;
+        const int am = swap ? bn : 1, akk = swap ? bk : ak, bkk = swap ? ak : bk, bnn = swap ? 1 : bn;
+        const int cm = swap ? cn : 1, cnn = swap ? 1 : cn;
+        const int mt = (Mt + 16 * RM - 1) / (16 * RM), nt = (Nt + 8 * RN - 1) / (8 * RN);
+        const int tiles = mt * nt;
+        const int items = (ACC ? 1 : G) * nc * tiles;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int g = lane >> 2, t = lane & 3;
+        for (int it = warp; it < items; it += NW) {
+                const int tile = it % tiles;
+                const int gc = it / tiles;
+                const int tm = tile % mt, tn = tile / mt;
+                const int c = ACC ? gc : gc % nc;
+                const int g0 = ACC ? 0 : gc / nc;
+                const int g1 = ACC ? G : g0 + 1;
+                const int m0 = tm * 16 * RM, n0 = tn * 8 * RN;
+                float d[RM][RN][4];
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int j = 0; j < RN; ++j)
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) d[i][j][q] = 0.f;
+                for (int gg = g0; gg < g1; ++gg) {
+                        const float *op = ops + opoff[gg];
+                        const float *tin = in + gg * in_gs;
+                        const float *Ab = ax == 0 ? op : tin + c * a_cs;
+                        const float *Bb = ax == 0 ? tin : op;
+                        warp_tile_tf32x3<RM, RN>(d, swap ? Bb : Ab, am, akk, swap ? Ab : Bb, bkk, bnn, K,
+                                                 Mt, Nt, m0, n0, g, t);
+                }
+                const float sc = (!ACC && scale) ? scale[g0] : 1.f;
+                float *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs;
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int r = 0; r < 2; ++r) {
+                                const int mc = m0 + 16 * i + 8 * r + g;
+                                if (mc >= Mt) continue;
+#pragma unroll
+                                for (int j = 0; j < RN; ++j)
+#pragma unroll
+                                        for (int h = 0; h < 2; ++h) {
+                                                const int ncol = n0 + 8 * j + 2 * t + h;
+                                                if (ncol >= Nt) continue;
+                                                float *cp = Cb + mc * cm + ncol * cnn;
+                                                const float v = d[i][j][2 * r + h];
+                                                *cp = ACC ? *cp + v : sc * v;
+                                        }
+                        }
+        }
+}
+
+template <bool ACC, int NW>
+__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
+                                              const int64_t *opoff, const float *__restrict__ ops,
+                                              const float *in, int in_gs, float *out, int out_gs,
+                                              const float *scale)
+{
+        const int M = ax == 0 ? rows : ax == 1 ? w[0] : w[0] * w[1];
+        const int N = ax == 0 ? w[1] * w[2] : rows;
+        // padded work of the two orientations (16 x 8 granules)
+        const int64_t pw0 = (int64_t) ((M + 15) / 16) * ((N + 7) / 8);
+        const int64_t pw1 = (int64_t) ((N + 15) / 16) * ((M + 7) / 8);
+        const bool swap = pw1 < pw0;
+        const int Mt = swap ? N : M, Nt = swap ? M : N;
+        if (Mt <= 16)
+                grouped_stage_f32_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                   out_gs, scale, swap);
+        else if (Nt <= 8)
+                grouped_stage_f32_t<ACC, 4, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                   out_gs, scale, swap);
+        else
+                grouped_stage_f32_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                   out_gs, scale, swap);
+}
+
+// Shared buffer capacities (elements) of a configuration for element type T:
+// the output tile is the plan's; FP32 fits twice the staged block and
+// intermediates in the same bytes.
+template <class Cfg, class T>
+struct Caps {
+        static constexpr int kOut = Cfg::kOut;
+        static constexpr int kPsi = Cfg::kPsi * (int) (sizeof(double) / sizeof(T));
+        static constexpr int kW = Cfg::kW * (int) (sizeof(double) / sizeof(T));
+};
+
+template <class Cfg, class T>
+constexpr size_t smem_bytes_t()
+{
+        return sizeof(T) * (Caps<Cfg, T>::kOut + Caps<Cfg, T>::kPsi + Caps<Cfg, T>::kW + kGMax) +
+               sizeof(int64_t) * 3 * kGMax + 64;
+}
+
+template <class Cfg, class T>
 __global__ void __launch_bounds__(Cfg::kThreads, Cfg::kMinBlocks)
-heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
-                 const double *__restrict__ ops, const int64_t *__restrict__ blk_off,
+heff_kernel(const T *__restrict__ x, double *__restrict__ y,
+                 const T *__restrict__ ops, const int64_t *__restrict__ blk_off,
                  const int4 *__restrict__ edims, const HeffUnit *__restrict__ units, int n_units,
                  const int *__restrict__ pair_ptr, const HeffPair *__restrict__ pairs,
                  const HeffTask *__restrict__ tasks, int *counter, int *err)
 {
         extern __shared__ __align__(16) unsigned char smem_raw[];
-        double *OUT = reinterpret_cast<double *>(smem_raw);
+        using C = Caps<Cfg, T>;
+        T *OUT = reinterpret_cast<T *>(smem_raw);
         constexpr int kThreads = Cfg::kThreads, NW = Cfg::kThreads / 32;
-        double *PSI = OUT + Cfg::kOut;
-        double *W = PSI + Cfg::kPsi;
-        double *PREF = W + Cfg::kW;
+        T *PSI = OUT + C::kOut;
+        T *W = PSI + C::kPsi;
+        T *PREF = W + C::kW;
         int64_t *OPOFF = reinterpret_cast<int64_t *>(PREF + kGMax);   // [3][kGMax]
         int *UNIT = reinterpret_cast<int *>(OPOFF + 3 * kGMax);
         const int tid = threadIdx.x;
@@ -256,7 +438,7 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                 const int ext[3] = {un.at, un.bt, un.ct};
                 const int row0[3] = {un.a0, un.b0, un.c0};
                 const int st = ext[0] * ext[1] * ext[2];
-                for (int e = tid; e < st; e += kThreads) OUT[e] = 0.0;
+                for (int e = tid; e < st; e += kThreads) OUT[e] = T(0);
                 __syncthreads();
                 for (int p = un.p0; p < un.p1; ++p) {
                         const HeffPair pr = pairs[p];
@@ -272,18 +454,18 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                         const int s0 = w0[0] * w0[1] * w0[2];
                         const int s1 = w1[0] * w1[1] * w1[2];
                         const int s2 = nst == 3 ? w2[0] * w2[1] * w2[2] : 0;
-                        if (s1 + s2 > Cfg::kW) {
+                        if (s1 + s2 > C::kW) {
                                 if (tid == 0) atomicExch(err, 3);
                                 return;
                         }
-                        const double *xin = x + blk_off[pr.old];
-                        const double *in0 = xin;
-                        if (s0 <= Cfg::kPsi) {
+                        const T *xin = x + blk_off[pr.old];
+                        const T *in0 = xin;
+                        if (s0 <= C::kPsi) {
                                 for (int e = tid; e < s0; e += kThreads) PSI[e] = xin[e];
                                 in0 = PSI;
                         }
-                        const int G = min(kGMax, Cfg::kW / (s1 + s2));
-                        double *W1 = W, *W2 = W + G * s1;
+                        const int G = min(kGMax, C::kW / (s1 + s2));
+                        T *W1 = W, *W2 = W + G * s1;
                         const int nterm = pr.t1 - pr.t0;
                         for (int t0 = 0; t0 < nterm; t0 += G) {
                                 const int g = min(G, nterm - t0);
@@ -291,7 +473,7 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                                         const HeffTask &tk = tasks[pr.t0 + t0 + tid];
                                         for (int s = 0; s < 3; ++s)
                                                 OPOFF[s * kGMax + tid] = tk.op_off[ax[s]] + row0[ax[s]];
-                                        PREF[tid] = tk.pref;
+                                        PREF[tid] = (T) tk.pref;
                                 }
                                 __syncthreads();
                                 if (nst == 3) {
@@ -324,8 +506,8 @@ heff_fp64_kernel(const double *__restrict__ x, double *__restrict__ y,
                         const int c = t / ext[1];
                         double *dst = yn + (row0[0] + a) +
                                       (int64_t) dn[0] * ((row0[1] + b) + (int64_t) dn[1] * (row0[2] + c));
-                        if (un.split) atomicAdd(dst, OUT[e]);
-                        else *dst = OUT[e];
+                        if (un.split) atomicAdd(dst, (double) OUT[e]);
+                        else *dst = (double) OUT[e];
                 }
                 __syncthreads();
         }
@@ -734,38 +916,72 @@ int tile_plan(HostPlan &hp, int cfg)
         return T3NS_OK;
 }
 
-template <class Cfg>
-static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const double *x, double *y,
-                      cudaStream_t s)
+template <class Cfg, class T>
+static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const T *x, const T *ops,
+                      double *y, cudaStream_t s)
 {
-        static bool attr_set = false;   // per configuration (one instantiation each)
+        static bool attr_set = false;   // per instantiation
         if (!attr_set) {
-                T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_fp64_kernel<Cfg>,
+                T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_kernel<Cfg, T>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int) smem_bytes<Cfg>()));
+                                                   (int) smem_bytes_t<Cfg, T>()));
                 attr_set = true;
         }
-        heff_fp64_kernel<Cfg><<<dt.grid, Cfg::kThreads, smem_bytes<Cfg>(), s>>>(
-                x, y, dp.ops, dp.blk_off, dp.edims, dt.units, dt.n_units, dt.pair_ptr, dt.pairs,
+        heff_kernel<Cfg, T><<<dt.grid, Cfg::kThreads, smem_bytes_t<Cfg, T>(), s>>>(
+                x, y, ops, dp.blk_off, dp.edims, dt.units, dt.n_units, dt.pair_ptr, dt.pairs,
                 dp.tasks, dp.counter, dp.err);
         T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
+}
+
+__global__ void to_f32_kernel(const double *__restrict__ a, float *__restrict__ b, int64_t n)
+{
+        for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+             i += (int64_t) gridDim.x * blockDim.x)
+                b[i] = (float) a[i];
+}
+
+int convert_to_f32(const double *a, float *b, int64_t n, cudaStream_t s)
+{
+        if (n <= 0) return T3NS_OK;
+        const int grid = (int) std::min<int64_t>((n + 255) / 256, 148 * 16);
+        to_f32_kernel<<<grid, 256, 0, s>>>(a, b, n);
+        T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
+}
+
+int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
+                int *launches)
+{
+        const DeviceTiles &dt = dp.tiles[dp.active];
+        if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
+        const bool split = precision == T3NS_PREC_3XTF32;
+        if (split && (!dp.ops32 || !dp.x32))
+                return set_error(T3NS_E_ARG, "matvec: split precision is not set up on this plan");
+        if (precision != T3NS_PREC_FP64 && !split)
+                return set_error(T3NS_E_ARG, "matvec: unsupported precision");
+        T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
+        if (launches) *launches = 0;
+        if (dt.n_units == 0) return T3NS_OK;
+        if (split) T3NS_TRY(convert_to_f32(x, dp.x32, dp.size, s));
+        T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
+        static_assert(kNumCfgs == 2, "one launch branch per configuration");
+        int rc;
+        if (split)
+                rc = dp.active == 0 ? launch_cfg<CfgLarge, float>(dp, dt, dp.x32, dp.ops32, y, s)
+                                    : launch_cfg<CfgSmall, float>(dp, dt, dp.x32, dp.ops32, y, s);
+        else
+                rc = dp.active == 0 ? launch_cfg<CfgLarge, double>(dp, dt, x, dp.ops, y, s)
+                                    : launch_cfg<CfgSmall, double>(dp, dt, x, dp.ops, y, s);
+        T3NS_TRY(rc);
+        if (launches) *launches = split ? 2 : 1;
         return T3NS_OK;
 }
 
 int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStream_t s,
                      int *launches)
 {
-        const DeviceTiles &dt = dp.tiles[dp.active];
-        if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
-        T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
-        if (launches) *launches = 0;
-        if (dt.n_units == 0) return T3NS_OK;
-        T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
-        static_assert(kNumCfgs == 2, "one launch branch per configuration");
-        T3NS_TRY(dp.active == 0 ? launch_cfg<CfgLarge>(dp, dt, x, y, s)
-                                : launch_cfg<CfgSmall>(dp, dt, x, y, s));
-        if (launches) *launches = 1;
-        return T3NS_OK;
+        return launch_heff(dp, T3NS_PREC_FP64, x, y, s, launches);
 }
 
 int launch_heff_diag(const DevicePlan &dp, double *diag, cudaStream_t s)

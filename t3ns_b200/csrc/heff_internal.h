@@ -101,6 +101,8 @@ struct DevicePlan {
         int nblocks = 0;
         int64_t size = 0;
         double *ops = nullptr;
+        float *ops32 = nullptr;                   // FP32 copy for the split-precision matvec
+        float *x32 = nullptr;                     // FP32 input staging
         int64_t *blk_off = nullptr;
         int4 *edims = nullptr;
         int *task_ptr = nullptr;
@@ -118,6 +120,10 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp);
 int tile_plan(HostPlan &hp, int cfg);
 int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStream_t s,
                      int *launches);
+// The matvec in precision T3NS_PREC_FP64 or T3NS_PREC_3XTF32 (FP64 in and out).
+int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
+                int *launches);
+int convert_to_f32(const double *a, float *b, int64_t n, cudaStream_t s);
 int launch_heff_diag(const DevicePlan &dp, double *diag, cudaStream_t s);
 
 }  // namespace t3ns

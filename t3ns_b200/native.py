@@ -62,7 +62,7 @@ class HeffStats(C.Structure):
 
 class DavidsonInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("max_vecs", C.c_int), ("d_energy", C.c_double),
-                ("residual", C.c_double), ("seconds", C.c_double)]
+                ("residual", C.c_double), ("seconds", C.c_double), ("fp64_iterations", C.c_int)]
 
 
 _lib = None
@@ -222,6 +222,9 @@ class HeffPlan:
         check(self.lib.t3ns_heff_matvec_host(self.h, _ptr(x, C.c_double), _ptr(y, C.c_double)),
               "matvec_host")
         return y
+
+    def set_precision(self, precision: int):
+        check(self.lib.t3ns_heff_set_precision(self.h, precision), "set_precision")
 
     def set_config(self, config: int):
         check(self.lib.t3ns_heff_set_config(self.h, config), "set_config")

@@ -123,3 +123,49 @@ def test_autotune_picks_fastest_and_caches(torch_cuda):
     assert again.autotune(reps=1, force=False) == [0.0, 0.0]   # bucket known: not re-timed
     again.close()
     plan.close()
+
+
+# Split precision (3xTF32 products of FP32 data, FP32 accumulation): the matvec
+# error against the reference's FP64 output comes from FP32 rounding of the
+# data (2^-24), the dropped lo*lo product terms (~2^-22 each) and FP32 sums
+# over three contraction stages; measured 1.8e-6 - 1.9e-6 relative
+# (norm-wise) on the D=512 steps, so 5e-6 is the stated tolerance.
+SPLIT_RTOL = 5e-6
+
+
+@pytest.mark.parametrize("config", [0, 1])
+@pytest.mark.parametrize("path", STEPS[::2], ids=lambda p: "/".join(p.split("/")[-2:]))
+def test_split_precision_matvec_error(path, config, torch_cuda):
+    from t3ns_b200.native import T3NS_PREC_3XTF32
+    s = read_step(path)
+    plan = HeffPlan(StepDesc(s), T3NS_PREC_3XTF32)
+    plan.set_config(config)
+    for v in range(2):
+        err = _rel(plan.matvec_host(s[f"x{v}"]), s[f"y{v}"])
+        assert err <= SPLIT_RTOL, err
+    assert plan.last_launches() == 2      # FP32 conversion of x + the matvec
+    plan.close()
+
+
+@pytest.mark.parametrize("path", [p for p in STEPS if "eig.energy" in read_step(p)],
+                         ids=lambda p: "/".join(p.split("/")[-2:]))
+def test_split_precision_davidson_defect_corrected(path, torch_cuda):
+    """Split-precision iterations followed by FP64 defect correction reach the
+    reference's Davidson energy to 1e-8 Ha with an FP64 residual below tol."""
+    from t3ns_b200.native import T3NS_PREC_3XTF32
+    s = read_step(path)
+    tol = float(s["eig.tol"][0])
+    plan = HeffPlan(StepDesc(s), T3NS_PREC_3XTF32)
+    res = s["eig.guess"].copy()
+    e, ret, info = plan.davidson_host(res, s["diag"], tol=tol, max_its=int(s["eig.max_its"][0]),
+                                      max_vecs=int(s["eig.max_vecs"][0]),
+                                      keep=int(s["eig.keep"][0]))
+    plan.close()
+    if int(s["eig.ret"][0]) == 0:
+        assert ret == 0
+    assert abs(e - float(s["eig.energy"][0])) <= ENERGY_TOL
+    assert info["fp64_iterations"] >= 1
+    fp64 = HeffPlan(StepDesc(s))
+    r = fp64.matvec_host(res) - e * res
+    assert np.linalg.norm(r) <= tol * 1.01
+    fp64.close()
