@@ -2,8 +2,14 @@
 
 One step = one matvec Psi' = Heff Psi over one optimisation step of the
 synthetic 24-orbital quantum-chemistry Hamiltonian at D=512 (U1 x SU2,
-SITE_SIZE 2; step files captured from the reference sweep, operator values
-and schedule exactly as the reference builds them).
+SITE_SIZE 2): block structure, instruction set and schedule captured from
+the reference sweep; the operator values (0.9 GB, too large to ship) are
+drawn from a fixed seed, which leaves cost and schedule unchanged.
+
+Besides the FP64 line it reports the split-precision (3xTF32) matvec on the
+same step (`split_precision`) and whole sweeps of the reference driver
+linked against the drop-in with FP64 and with split-precision matvecs plus
+FP64 defect correction (`sweep`: sweep seconds and final-energy difference).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -21,6 +27,7 @@ import argparse
 import glob
 import json
 import os
+import re
 import subprocess
 import sys
 import time
@@ -174,6 +181,31 @@ def run_engine(args, rank, world):
     t_total = float(sum(t_steps))
     launches = plan.last_launches() * args.steps
 
+    # split precision (3xTF32) on the same step: time, and error against FP64
+    from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_FP64
+    y64 = y.clone()
+    plan.set_precision(T3NS_PREC_3XTF32)
+    split_tune = plan.autotune(reps=1)
+    for _ in range(args.warmup):
+        plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
+    torch.cuda.synchronize()
+    split_times = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
+        e1.record(stream)
+        split_times.append((e0, e1))
+    torch.cuda.synchronize()
+    t_split = float(sum(a.elapsed_time(b) * 1e-3 for a, b in split_times))
+    split_err = float((y - y64).norm() / y64.norm())
+    split_cfg = plan.config()
+    plan.set_precision(T3NS_PREC_FP64)
+    plan.autotune(reps=1, force=False)
+    y.copy_(y64)
+
     # e2e: host buffers (pinned) through the C-ABI host entry point
     xh = x.cpu().pin_memory()
     yh = torch.empty_like(xh).pin_memory()
@@ -219,9 +251,55 @@ def run_engine(args, rank, world):
                                     "peak; MEASURED_PEAKS.json has no FP64 figure)"},
         "e2e": {"value": flops * args.steps * world / t_e2e / 1e12, "unit": UNIT,
                 "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "split_precision": {"value": flops * args.steps * world / t_split / 1e12, "unit": UNIT,
+                            "ms_per_step": 1e3 * t_split / args.steps,
+                            "speedup_vs_fp64": t_total / t_split,
+                            "rel_err_vs_fp64": split_err, "kernel_config": split_cfg,
+                            "autotune_ms": split_tune,
+                            "arithmetic": "3xTF32 products of FP32 data, FP32 accumulation"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    return out
+
+
+def sweep_comparison(timeout=900):
+    """Whole sweeps of the reference's own driver linked against the drop-in,
+    once with the FP64 matvec and once with the split-precision (3xTF32)
+    matvec plus FP64 defect correction: sweep seconds of each and the
+    final-energy difference.  Cases: the Hubbard tree (D=128, SITE_SIZE 2,
+    6 sweeps; E_exact = -6.194800043519880) and the synthetic 12-orbital QC
+    Hamiltonian (D=128, 2 sweeps).  None if the driver is not built."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "t3ns_run_dropin")
+    if not os.path.exists(exe):
+        return None
+    from t3ns_b200.workloads import synthetic_qc_fcidump
+    net = os.path.join(ROOT, "tests", "golden", "networks")
+    fcid = synthetic_qc_fcidump(os.path.join("/tmp", "t3ns_bench_qc12.FCIDUMP"), 12, 12, 0, 72)
+    cases = {
+        "hubbard10_D128_6sweeps": ["--net", os.path.join(net, "t3ns_10.netw"), "--inter",
+                                   "NN_HUBBARD ( t = 1 U = 4 )", "--symm", "Z2,U1,SU2", "--ts",
+                                   "0,10,0", "--regime", "128,128,0,2,1e-5,100,6,1e-8,0"],
+        "qc12_D128_2sweeps": ["--net", os.path.join(net, "t3ns_12.netw"), "--inter", fcid,
+                              "--symm", "Z2,U1,SU2", "--ts", "0,12,0",
+                              "--regime", "128,128,0,2,1e-5,100,2,1e-8,0"],
+    }
+    out = {}
+    for name, args in cases.items():
+        rec = {}
+        for prec in ("fp64", "3xtf32"):
+            env = dict(os.environ, T3NS_B200_PRECISION=prec, OMP_NUM_THREADS="8",
+                       OPENBLAS_NUM_THREADS="1")
+            r = subprocess.run([exe, *args, "--init", "c"], capture_output=True, text=True,
+                               env=env, timeout=timeout)
+            if r.returncode != 0:
+                return {"error": f"{name} {prec}: exit {r.returncode}"}
+            e = float(re.findall(r"FINAL_ENERGY (\S+)", r.stdout)[-1])
+            t = float(re.findall(r"SWEEP_SECONDS (\S+)", r.stdout)[-1])
+            rec[prec] = {"sweep_seconds": t, "energy": e}
+        rec["speedup_mixed_vs_fp64"] = rec["fp64"]["sweep_seconds"] / rec["3xtf32"]["sweep_seconds"]
+        rec["abs_dE_mixed_vs_fp64"] = abs(rec["3xtf32"]["energy"] - rec["fp64"]["energy"])
+        out[name] = rec
     return out
 
 
@@ -274,6 +352,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="skip the whole-sweep FP64 vs split-precision comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -326,6 +406,8 @@ def main():
                                                  "of the same step" % cb["stride"]}
             else:
                 out["cpu_baseline"] = None
+        if not args.no_sweep:
+            out["sweep"] = sweep_comparison()
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

@@ -489,7 +489,8 @@ static int precision_from_env(void)
         if (!p || !strcmp(p, "fp64")) return T3NS_PREC_FP64;
         if (!strcmp(p, "3xtf32")) return T3NS_PREC_3XTF32;
         if (!strcmp(p, "bf16x3")) return T3NS_PREC_BF16X3;
-        return T3NS_PREC_FP64;
+        fprintf(stderr, "t3ns drop-in: T3NS_B200_PRECISION=%s is not one of fp64, 3xtf32, bf16x3\n", p);
+        exit(EXIT_FAILURE);
 }
 
 void init_Heffdata(struct Heffdata *data, const struct rOperators *Operators,

@@ -92,6 +92,17 @@ def test_sweep_energy_hubbard_config1():
 
 
 @pytest.mark.gpu
+def test_sweep_energy_hubbard_config1_split_precision():
+    """Config 1 with split-precision (3xTF32) matvecs and FP64 defect
+    correction in every Davidson solve: the final energy stays within 1e-8 Ha
+    of exact diagonalisation."""
+    need(RUN_DROPIN)
+    args = HUB10 + ["--regime", "128,128,0,2,1e-5,100,6,1e-8,0", "--init", "c"]
+    out = run(RUN_DROPIN, args, {"T3NS_B200_PRECISION": "3xtf32"})
+    assert abs(energy(out) - (-6.194800043519880)) <= 1e-8
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("net", ["10_T3NS", "10_DMRG"])
 @pytest.mark.parametrize("symm,ts", [("Z2,U1,SU2", "0,14,0"), ("Z2,U1,SU2,D2h", "0,14,0,0"),
                                      ("Z2,U1,U1", "0,7,7")])
