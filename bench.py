@@ -304,10 +304,10 @@ def sweep_comparison(timeout=900):
 
 
 def traffic_from_profile(workload_path):
-    """DRAM bytes (read + write) of one heff_fp64_kernel launch on this
-    workload, from the ncu capture summarised under profiles/ (None if that
-    workload has not been profiled)."""
-    p = os.path.join(ROOT, "profiles", "heff_fp64_kernel_traffic.json")
+    """DRAM bytes (read + write) of one FP64 heff_kernel launch (kernel
+    configuration 0) on this workload, from the ncu capture summarised under
+    profiles/ (None if that workload has not been profiled)."""
+    p = os.path.join(ROOT, "profiles", "heff_kernel_traffic.json")
     if not os.path.exists(p):
         return None
     rec = json.load(open(p)).get(os.path.basename(workload_path))

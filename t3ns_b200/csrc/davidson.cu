@@ -20,10 +20,12 @@
 // fixed order.  The host reads 4 doubles per iteration to decide whether to
 // stop.
 #include <chrono>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <cmath>
 #include <functional>
+#include <string>
 #include <vector>
 
 #include "common.h"
@@ -67,11 +69,20 @@ __device__ void block_sums(double (&v)[NV], double *out)
         __syncthreads();
 }
 
-// partials[b * ncols + j] = sum over the rows of block b of V[i, j] * t[i]
+// Counts and columns that depend on the current basis size m are read on
+// the device (dm; nullptr means m = 0), so one captured graph serves every
+// iteration: ncols = m + nadd, and a vector argument flagged "at m" is
+// column m of its matrix (leading dimension ld).
+__device__ __forceinline__ int dev_m(const int *dm) { return dm ? *dm : 0; }
+
+// partials[b * ncols + j] = sum over the rows of block b of V[i, j] * t[i],
+// ncols = m + nadd, t = tb (or column m of tb when t_at_m)
 __global__ void __launch_bounds__(kRedThreads)
-dots_kernel(const double *__restrict__ V, int64_t ld, int ncols,
-            const double *__restrict__ t, int64_t n, double *__restrict__ partials)
+dots_kernel(const double *__restrict__ V, int64_t ld, const int *dm, int nadd,
+            const double *__restrict__ tb, int t_at_m, int64_t n, double *__restrict__ partials)
 {
+        const int ncols = dev_m(dm) + nadd;
+        const double *__restrict__ t = tb + (t_at_m ? (int64_t) dev_m(dm) * ld : 0);
         for (int j0 = 0; j0 < ncols; j0 += kChunk) {
                 double acc[kChunk];
 #pragma unroll
@@ -91,10 +102,14 @@ dots_kernel(const double *__restrict__ V, int64_t ld, int ncols,
         }
 }
 
-// out[j * out_stride] = scale * sum_b partials[b * ncols + j]   (fixed order)
-__global__ void reduce_partials_kernel(const double *__restrict__ partials, int nblk, int ncols,
-                                       double *__restrict__ out, int out_stride, double scale)
+// out[j * out_stride] = scale * sum_b partials[b * ncols + j]   (fixed order),
+// ncols = m + nadd; out = ob (or ob + m * out_col when out_col != 0)
+__global__ void reduce_partials_kernel(const double *__restrict__ partials, int nblk,
+                                       const int *dm, int nadd, double *__restrict__ ob,
+                                       int64_t out_col, int out_stride, double scale)
 {
+        const int ncols = dev_m(dm) + nadd;
+        double *__restrict__ out = ob + (int64_t) dev_m(dm) * out_col;
         for (int j = threadIdx.x; j < ncols; j += blockDim.x) {
                 double s = 0;
                 for (int b = 0; b < nblk; ++b) s += partials[b * ncols + j];
@@ -104,10 +119,11 @@ __global__ void reduce_partials_kernel(const double *__restrict__ partials, int 
 
 // t[i] -= sum_j V[i, j] coef[j]; partials[b] = block sum of t[i]^2 afterwards
 __global__ void __launch_bounds__(kRedThreads)
-gs_update_kernel(const double *__restrict__ V, int64_t ld, int ncols,
+gs_update_kernel(const double *__restrict__ V, int64_t ld, const int *dm,
                  const double *__restrict__ coef, double *__restrict__ t, int64_t n,
                  double *__restrict__ partials)
 {
+        const int ncols = dev_m(dm);
         __shared__ double c[64];
         for (int j = threadIdx.x; j < ncols; j += blockDim.x) c[j] = coef[j];
         __syncthreads();
@@ -138,12 +154,14 @@ norm2_kernel(const double *__restrict__ t, int64_t n, double *__restrict__ parti
         if (threadIdx.x == 0) partials[blockIdx.x] = out[0];
 }
 
-// out[i] = t[i] / ||t||, with ||t||^2 = sum of the nblk partials (each block
-// reduces them itself, in the same order)
+// column m of V and out2 (if not null) = t / ||t||, with ||t||^2 = sum of
+// the nblk partials (each block reduces them itself, in the same order)
 __global__ void __launch_bounds__(kRedThreads)
-normalize_kernel(const double *__restrict__ t, double *__restrict__ out, int64_t n,
+normalize_kernel(const double *__restrict__ t, double *__restrict__ V, int64_t ld,
+                 const int *dm, double *__restrict__ out2, int64_t n,
                  const double *__restrict__ partials, int nblk)
 {
+        double *__restrict__ out = V + (int64_t) dev_m(dm) * ld;
         __shared__ double inv;
         if (threadIdx.x == 0) {
                 double s = 0;
@@ -153,8 +171,28 @@ normalize_kernel(const double *__restrict__ t, double *__restrict__ out, int64_t
         __syncthreads();
         const double a = inv;
         for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+             i += (int64_t) gridDim.x * blockDim.x) {
+                const double v = t[i] * a;
+                out[i] = v;
+                if (out2) out2[i] = v;
+        }
+}
+
+// column m of VA = y
+__global__ void __launch_bounds__(kRedThreads)
+store_column_kernel(const double *__restrict__ y, double *__restrict__ VA, int64_t ld,
+                    const int *dm, int64_t n)
+{
+        double *__restrict__ out = VA + (int64_t) dev_m(dm) * ld;
+        for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
              i += (int64_t) gridDim.x * blockDim.x)
-                out[i] = t[i] * a;
+                out[i] = y[i];
+}
+
+// m <- m + add, or m <- set when set >= 0
+__global__ void set_m_kernel(int *dm, int add, int set)
+{
+        *dm = set >= 0 ? set : *dm + add;
 }
 
 // result = V y, t = VA y - theta result; partials[b*3 + {0,1,2}] =
@@ -162,11 +200,12 @@ normalize_kernel(const double *__restrict__ t, double *__restrict__ out, int64_t
 // (cutoff kDiagCutoff), i.e. calculate_residue and the reductions of the
 // preconditioner fused in one pass.
 __global__ void __launch_bounds__(kRedThreads)
-ritz_kernel(const double *__restrict__ V, const double *__restrict__ VA, int64_t ld, int m,
+ritz_kernel(const double *__restrict__ V, const double *__restrict__ VA, int64_t ld, const int *dm,
             const double *__restrict__ y, const double *__restrict__ theta_p,
             const double *__restrict__ diag, double *__restrict__ result,
             double *__restrict__ t, int64_t n, double *__restrict__ partials)
 {
+        const int m = dev_m(dm);
         __shared__ double c[64];
         for (int j = threadIdx.x; j < m; j += blockDim.x) c[j] = y[j];
         __syncthreads();
@@ -260,10 +299,11 @@ deflate_kernel(double *__restrict__ V, int64_t ld, int mcols, const double *__re
 // columns of Z (leading dimension ld).  Parallel cyclic Jacobi with
 // round-robin pairing (Golub & Van Loan, Alg. 8.4.3 / 8.4.4); one CTA.
 // status: 0 converged, 1 no convergence within the sweep limit.
-__global__ void jacobi_eig_kernel(const double *__restrict__ S, int ld, int m,
+__global__ void jacobi_eig_kernel(const double *__restrict__ S, int ld, const int *dm,
                                   double *__restrict__ Z, double *__restrict__ w,
                                   int *__restrict__ status)
 {
+        const int m = dev_m(dm);
         __shared__ double A[kMaxVecs][kMaxVecs + 1];
         __shared__ double Q[kMaxVecs][kMaxVecs + 1];
         __shared__ double cs[kMaxVecs / 2][2];
@@ -374,12 +414,15 @@ __global__ void jacobi_eig_kernel(const double *__restrict__ S, int ld, int m,
 struct DavidsonBuffers {
         double *V = nullptr, *VA = nullptr, *t = nullptr, *S = nullptr, *Z = nullptr,
                *w = nullptr, *partials = nullptr, *coef = nullptr, *scal = nullptr;
+        double *vin = nullptr, *vout = nullptr;   // fixed matvec operands
         int *status = nullptr;
+        int *dm = nullptr;                          // current basis size
         double *host_scal = nullptr;   // pinned
         ~DavidsonBuffers()
         {
                 cudaFree(V); cudaFree(VA); cudaFree(t); cudaFree(S); cudaFree(Z); cudaFree(w);
                 cudaFree(partials); cudaFree(coef); cudaFree(scal); cudaFree(status);
+                cudaFree(vin); cudaFree(vout); cudaFree(dm);
                 if (host_scal) cudaFreeHost(host_scal);
         }
 };
@@ -413,7 +456,8 @@ using DevMatvec = std::function<int(const double *, double *, cudaStream_t)>;
 // whose residual levels off at the matvec's rounding).
 static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, double *energy,
                          int max_vecs, int keep, double tol, int max_its, const double *d_diag,
-                         t3ns_davidson_info *info, cudaStream_t s, int stall = 0)
+                         t3ns_davidson_info *info, cudaStream_t s, int stall = 0,
+                         bool use_graphs = false)
 {
         const auto t_start = std::chrono::steady_clock::now();
         if (max_vecs > kMaxVecs || keep > 4 || keep < 1 || keep >= max_vecs || max_vecs < 3)
@@ -431,6 +475,9 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
         T3NS_CUDA_TRY(cudaMalloc(&b.coef, sizeof(double) * 64));
         T3NS_CUDA_TRY(cudaMalloc(&b.scal, sizeof(double) * 8));
         T3NS_CUDA_TRY(cudaMalloc(&b.status, sizeof(int)));
+        T3NS_CUDA_TRY(cudaMalloc(&b.dm, sizeof(int)));
+        T3NS_CUDA_TRY(cudaMalloc(&b.vin, sizeof(double) * n));
+        T3NS_CUDA_TRY(cudaMalloc(&b.vout, sizeof(double) * n));
         T3NS_CUDA_TRY(cudaMallocHost(&b.host_scal, sizeof(double) * 8));
         T3NS_CUDA_TRY(cudaMemsetAsync(b.S, 0, sizeof(double) * mv * mv, s));
         T3NS_CUDA_TRY(cudaMemcpyAsync(b.t, d_result, sizeof(double) * n,
@@ -440,52 +487,45 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
         bool stalled = false;
         double res = tol * 10, e_old = 0, d_e = tol * 10, best_res = 0;
         *energy = 0;
+        T3NS_CUDA_TRY(cudaMemsetAsync(b.dm, 0, sizeof(int), s));
 
-        auto column_of_S = [&](int col) -> int {
-                // S[i, col] = V_i . VA_col, i <= col
-                dots_kernel<<<G, T, 0, s>>>(b.V, n, col + 1, b.VA + (int64_t) col * n, n, b.partials);
-                reduce_partials_kernel<<<1, 64, 0, s>>>(b.partials, G, col + 1,
-                                                        b.S + (int64_t) col * mv, 1, 1.0);
-                T3NS_CUDA_TRY(cudaGetLastError());
-                return T3NS_OK;
+        // One iteration, with every m-dependent count and column read from
+        // b.dm on the device (so it can be captured once and replayed):
+        // new search vector (CGS2 + normalise), matvec, new column of S,
+        // Rayleigh-Ritz, deflation when the basis is full, Ritz vector and
+        // residual, the host's 4 doubles, preconditioner.
+        auto column_of_S = [&](const int *dm, int col) {
+                // S[i, c] = V_i . VA_c for i <= c, c = m (dm) or col (dm == nullptr)
+                dots_kernel<<<G, T, 0, s>>>(b.V, n, dm, dm ? 1 : col + 1,
+                                            b.VA + (dm ? 0 : (int64_t) col * n), dm ? 1 : 0, n,
+                                            b.partials);
+                reduce_partials_kernel<<<1, 64, 0, s>>>(b.partials, G, dm, dm ? 1 : col + 1,
+                                                        b.S + (dm ? 0 : (int64_t) col * mv),
+                                                        dm ? mv : 0, 1, 1.0);
         };
-        auto eigsolve = [&](int mm) -> int {
-                jacobi_eig_kernel<<<1, 256, 0, s>>>(b.S, mv, mm, b.Z, b.w, b.status);
-                T3NS_CUDA_TRY(cudaGetLastError());
-                return T3NS_OK;
-        };
-
-        while (res > tol && its < max_its && !stalled) {
-                double *vm = b.V + (int64_t) m * n;
-                if (m > 0) {
-                        for (int pass = 0; pass < 2; ++pass) {
-                                dots_kernel<<<G, T, 0, s>>>(b.V, n, m, b.t, n, b.partials);
-                                reduce_partials_kernel<<<1, 64, 0, s>>>(b.partials, G, m, b.coef, 1, 1.0);
-                                gs_update_kernel<<<G, T, 0, s>>>(b.V, n, m, b.coef, b.t, n, b.partials);
-                        }
-                } else {
-                        norm2_kernel<<<G, T, 0, s>>>(b.t, n, b.partials);
+        auto body = [&](bool deflate) -> int {
+                for (int pass = 0; pass < 2; ++pass) {
+                        dots_kernel<<<G, T, 0, s>>>(b.V, n, b.dm, 0, b.t, 0, n, b.partials);
+                        reduce_partials_kernel<<<1, 64, 0, s>>>(b.partials, G, b.dm, 0, b.coef, 0, 1, 1.0);
+                        gs_update_kernel<<<G, T, 0, s>>>(b.V, n, b.dm, b.coef, b.t, n, b.partials);
                 }
-                normalize_kernel<<<G, T, 0, s>>>(b.t, vm, n, b.partials, G);
+                normalize_kernel<<<G, T, 0, s>>>(b.t, b.V, n, b.dm, b.vin, n, b.partials, G);
                 T3NS_CUDA_TRY(cudaGetLastError());
-                T3NS_TRY(matvec(vm, b.VA + (int64_t) m * n, s));
-                T3NS_TRY(column_of_S(m));
-                ++m;
-                T3NS_TRY(eigsolve(m));
-                if (m == mv) {
+                T3NS_TRY(matvec(b.vin, b.vout, s));
+                store_column_kernel<<<G, T, 0, s>>>(b.vout, b.VA, n, b.dm, n);
+                column_of_S(b.dm, 0);
+                set_m_kernel<<<1, 1, 0, s>>>(b.dm, 1, -1);
+                jacobi_eig_kernel<<<1, 256, 0, s>>>(b.S, mv, b.dm, b.Z, b.w, b.status);
+                if (deflate) {
                         deflate_kernel<<<G, T, 0, s>>>(b.V, n, mv, b.Z, mv, keep, n);
                         deflate_kernel<<<G, T, 0, s>>>(b.VA, n, mv, b.Z, mv, keep, n);
-                        T3NS_CUDA_TRY(cudaGetLastError());
-                        m = 0;
-                        while (m < keep) {
-                                T3NS_TRY(column_of_S(m));
-                                ++m;
-                        }
-                        T3NS_TRY(eigsolve(m));
+                        set_m_kernel<<<1, 1, 0, s>>>(b.dm, 0, keep);
+                        for (int c = 0; c < keep; ++c) column_of_S(nullptr, c);
+                        jacobi_eig_kernel<<<1, 256, 0, s>>>(b.S, mv, b.dm, b.Z, b.w, b.status);
                 }
-                ritz_kernel<<<G, T, 0, s>>>(b.V, b.VA, n, m, b.Z, b.w, d_diag, d_result, b.t, n,
+                ritz_kernel<<<G, T, 0, s>>>(b.V, b.VA, n, b.dm, b.Z, b.w, d_diag, d_result, b.t, n,
                                             b.partials);
-                reduce_partials_kernel<<<1, 64, 0, s>>>(b.partials, G, 3, b.scal, 1, 1.0);
+                reduce_partials_kernel<<<1, 64, 0, s>>>(b.partials, G, nullptr, 3, b.scal, 0, 1, 1.0);
                 T3NS_CUDA_TRY(cudaGetLastError());
                 T3NS_CUDA_TRY(cudaMemcpyAsync(b.host_scal, b.scal, sizeof(double) * 3,
                                               cudaMemcpyDeviceToHost, s));
@@ -493,10 +533,61 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                                               cudaMemcpyDeviceToHost, s));
                 T3NS_CUDA_TRY(cudaMemcpyAsync(b.host_scal + 4, b.status, sizeof(int),
                                               cudaMemcpyDeviceToHost, s));
-                T3NS_CUDA_TRY(cudaStreamSynchronize(s));
+                precond_kernel<<<G, T, 0, s>>>(d_result, b.t, d_diag, b.scal, b.w, n);
+                T3NS_CUDA_TRY(cudaGetLastError());
+                return T3NS_OK;
+        };
+        // graph per iteration kind (plain / deflating), captured on first use
+        // after one eager iteration has run (the matvec's one-time set-up
+        // calls must not happen under capture)
+        cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+        auto release = [&]() {
+                for (auto &g : gexec)
+                        if (g) cudaGraphExecDestroy(g);
+        };
+        auto run_iteration = [&](bool deflate) -> int {
+                if (!use_graphs || its == 0) return body(deflate);
+                cudaGraphExec_t &ge = gexec[deflate ? 1 : 0];
+                if (!ge) {
+                        cudaGraph_t g = nullptr;
+                        T3NS_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                        const int rc = body(deflate);
+                        const cudaError_t ce = cudaStreamEndCapture(s, &g);
+                        if (rc != T3NS_OK) {
+                                if (g) cudaGraphDestroy(g);
+                                return rc;
+                        }
+                        if (ce != cudaSuccess)
+                                return set_error(T3NS_E_CUDA, std::string("davidson: capture: ") +
+                                                                      cudaGetErrorString(ce));
+                        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+                        cudaGraphDestroy(g);
+                        if (ie != cudaSuccess)
+                                return set_error(T3NS_E_CUDA, std::string("davidson: instantiate: ") +
+                                                                      cudaGetErrorString(ie));
+                }
+                T3NS_CUDA_TRY(cudaGraphLaunch(ge, s));
+                return T3NS_OK;
+        };
+
+        while (res > tol && its < max_its && !stalled) {
+                const bool deflate = m + 1 == mv;
+                const int rc = run_iteration(deflate);
+                if (rc != T3NS_OK) {
+                        release();
+                        return rc;
+                }
+                m = deflate ? keep : m + 1;
+                if (cudaStreamSynchronize(s) != cudaSuccess) {
+                        release();
+                        return set_error(T3NS_E_CUDA, "davidson: iteration failed");
+                }
                 int st = 0;
                 memcpy(&st, b.host_scal + 4, sizeof(int));
-                if (st != 0) return set_error(T3NS_E_EIG, "davidson: subspace eigensolver did not converge");
+                if (st != 0) {
+                        release();
+                        return set_error(T3NS_E_EIG, "davidson: subspace eigensolver did not converge");
+                }
                 res = sqrt(b.host_scal[0]);
                 if (its == 0 || res < 0.9 * best_res) {
                         best_res = res;
@@ -509,9 +600,8 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                 e_old = theta;
                 *energy = theta;
                 ++its;
-                precond_kernel<<<G, T, 0, s>>>(d_result, b.t, d_diag, b.scal, b.w, n);
-                T3NS_CUDA_TRY(cudaGetLastError());
         }
+        release();
         T3NS_CUDA_TRY(cudaStreamSynchronize(s));
         if (info) {
                 info->iterations = its;
@@ -536,17 +626,21 @@ int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
                         return launch_heff(h->dp, precision, x, y, st, &launches);
                 });
         };
+        // iterations replay captured CUDA graphs unless T3NS_B200_GRAPHS=0
+        const char *ge = getenv("T3NS_B200_GRAPHS");
+        const bool graphs = !ge || strcmp(ge, "0") != 0;
         if (h->precision == T3NS_PREC_FP64)
                 return davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy,
-                                     max_vecs, keep, tol, max_its, d_diag, info, s);
+                                     max_vecs, keep, tol, max_its, d_diag, info, s, 0, graphs);
         // split-precision iterations, then FP64 defect correction from their vector
         t3ns_davidson_info i1{}, i2{};
         const auto t0 = std::chrono::steady_clock::now();
         int rc = davidson_core(h->hp.size, matvec_in(h->precision), d_result, energy, max_vecs,
-                               keep, tol, max_its, d_diag, &i1, s, /*stall=*/4);
+                               keep, tol, max_its, d_diag, &i1, s, /*stall=*/4, graphs);
         if (rc < 0) return rc;
         rc = davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy, max_vecs,
-                           keep, tol, std::max(max_its - i1.iterations, 2), d_diag, &i2, s);
+                           keep, tol, std::max(max_its - i1.iterations, 2), d_diag, &i2, s, 0,
+                           graphs);
         if (rc < 0) return rc;
         if (info) {
                 *info = i2;
@@ -666,7 +760,7 @@ int t3ns_precondition_host(int64_t size, const double *result, double theta,
                 rc = set_error(T3NS_E_CUDA, "precondition: upload");
         if (rc == T3NS_OK) {
                 precond_sums_kernel<<<kRedBlocks, kRedThreads>>>(d_r, d_t, d_diag, d_theta, size, part);
-                reduce_partials_kernel<<<1, 64>>>(part, kRedBlocks, 3, scal, 1, 1.0);
+                reduce_partials_kernel<<<1, 64>>>(part, kRedBlocks, nullptr, 3, scal, 0, 1, 1.0);
                 precond_kernel<<<kRedBlocks, kRedThreads>>>(d_r, d_t, d_diag, scal, d_theta, size);
                 if (cudaGetLastError() != cudaSuccess ||
                     cudaMemcpy(vec_t, d_t, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -169,3 +169,38 @@ def test_split_precision_davidson_defect_corrected(path, torch_cuda):
     r = fp64.matvec_host(res) - e * res
     assert np.linalg.norm(r) <= tol * 1.01
     fp64.close()
+
+
+def test_davidson_graph_replay_matches_eager(torch_cuda, monkeypatch):
+    """Iterations replayed from captured CUDA graphs give bit-identical
+    energies, vectors and iteration counts to eager launches (the graphs hold
+    the same kernels; the basis size is read on the device)."""
+    cands = [p for p in STEPS if "eig.energy" in read_step(p)]
+    s = read_step(cands[len(cands) // 2])
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("T3NS_B200_GRAPHS", mode)
+        plan = HeffPlan(StepDesc(s))
+        res = s["eig.guess"].copy()
+        e, ret, info = plan.davidson_host(res, s["diag"], tol=float(s["eig.tol"][0]),
+                                          max_its=int(s["eig.max_its"][0]),
+                                          max_vecs=int(s["eig.max_vecs"][0]),
+                                          keep=int(s["eig.keep"][0]))
+        out[mode] = (e, ret, info["iterations"], res)
+        plan.close()
+    assert out["0"][:3] == out["1"][:3]
+    assert np.array_equal(out["0"][3], out["1"][3])
+
+
+def test_davidson_graphs_through_deflation(torch_cuda):
+    """A small subspace (max_vecs 4, keep 2) forces many deflations inside
+    the replayed graphs; the energy still matches the reference."""
+    cands = [p for p in STEPS if "eig.energy" in read_step(p)]
+    s = read_step(cands[0])
+    plan = HeffPlan(StepDesc(s))
+    res = s["eig.guess"].copy()
+    e, ret, info = plan.davidson_host(res, s["diag"], tol=float(s["eig.tol"][0]), max_its=400,
+                                      max_vecs=4, keep=2)
+    plan.close()
+    assert ret == 0 and info["iterations"] > 4
+    assert abs(e - float(s["eig.energy"][0])) <= ENERGY_TOL
