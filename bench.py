@@ -7,9 +7,11 @@ the reference sweep; the operator values (0.9 GB, too large to ship) are
 drawn from a fixed seed, which leaves cost and schedule unchanged.
 
 Besides the FP64 line it reports the split-precision (3xTF32) matvec on the
-same step (`split_precision`) and whole sweeps of the reference driver
-linked against the drop-in with FP64 and with split-precision matvecs plus
-FP64 defect correction (`sweep`: sweep seconds and final-energy difference).
+same step (`split_precision`), whole sweeps of the reference driver linked
+against the drop-in with FP64 and with split-precision matvecs plus FP64
+defect correction (`sweep`: sweep seconds and final-energy difference), and
+the engine's request loop under a Poisson stream of solves (`serving`:
+p50/p99 latency, solves/s).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -303,6 +305,54 @@ def sweep_comparison(timeout=900):
     return out
 
 
+def davidson_comparison(path=None, max_its=60, seed=7):
+    """One Davidson solve of a real D=512 step (the 24-orbital QC
+    Hamiltonian's step 6, 645,595 elements, operators as the reference built
+    them) from a seeded random guess, with FP64 matvecs and with
+    split-precision matvecs plus FP64 defect correction: seconds, iterations
+    and the energy difference.  None if the step is not present."""
+    path = path or os.path.join(ROOT, "oracle", "_ref", "captures", "qc24_D512", "step_006.t3c")
+    if not os.path.exists(path):
+        return None
+    from t3ns_b200.native import HeffPlan, StepDesc, T3NS_PREC_3XTF32, T3NS_PREC_FP64
+    from t3ns_b200.stepfile import read_step
+    s = read_step(path)
+    desc = StepDesc(s)
+    g0 = np.random.default_rng(seed).standard_normal(s["diag"].size)
+    g0 /= np.linalg.norm(g0)
+    out = {"step": os.path.relpath(path, ROOT), "psi_elems": int(s["diag"].size), "tol": 1e-5,
+           "max_its": max_its, "guess": "seeded N(0,1), normalised"}
+    for name, prec in (("fp64", T3NS_PREC_FP64), ("3xtf32", T3NS_PREC_3XTF32)):
+        plan = HeffPlan(desc, prec)
+        plan.autotune(reps=1, force=False)
+        g = g0.copy()
+        t0 = time.perf_counter()
+        e, rc, info = plan.davidson_host(g, s["diag"], tol=1e-5, max_its=max_its)
+        out[name] = {"seconds": time.perf_counter() - t0, "energy": e, "return": rc,
+                     "iterations": info["iterations"], "fp64_iterations": info["fp64_iterations"],
+                     "residual": info["residual"]}
+        plan.close()
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["3xtf32"]["seconds"]
+    out["abs_dE_mixed_vs_fp64"] = abs(out["3xtf32"]["energy"] - out["fp64"]["energy"])
+    return out
+
+
+def serving_stream():
+    """The engine's request loop under a Poisson stream of 128 independent
+    ground-state solves (mean 4 arrivals/s; solves drawn from the captured
+    Hubbard and 12-orbital QC steps, with the reference's operators), 8 GiB
+    admission budget, 4 in flight, split precision with FP64 defect
+    correction: p50/p99 latency and solves/s."""
+    from t3ns_b200.serving import Workload, request_steps, run_stream
+    steps = [p for p in request_steps() if "eig.energy" in Workload(p).step]
+    if not steps:
+        return None
+    _, summary = run_stream([Workload(p) for p in steps], n_requests=128, rate=4.0,
+                            budget_bytes=8 << 30, max_inflight=4, precision="3xtf32", seed=0)
+    summary["requests_from"] = "%d captured steps (Hubbard L=10 tree, 12-orbital QC)" % len(steps)
+    return summary
+
+
 def traffic_from_profile(workload_path):
     """DRAM bytes (read + write) of one FP64 heff_kernel launch (kernel
     configuration 0) on this workload, from the ncu capture summarised under
@@ -354,6 +404,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true",
                     help="skip the whole-sweep FP64 vs split-precision comparison")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the request-stream (serving) measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -407,7 +459,10 @@ def main():
             else:
                 out["cpu_baseline"] = None
         if not args.no_sweep:
+            out["davidson_D512"] = davidson_comparison()
             out["sweep"] = sweep_comparison()
+        if not args.no_serving:
+            out["serving"] = serving_stream()
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

@@ -154,9 +154,10 @@ typedef struct {
  * src/davidson.c:259-328: same subspace bound, deflation, Olsen-corrected
  * diagonal preconditioner with cutoff 1e-12, and stopping rule).  With the
  * plan in T3NS_PREC_3XTF32 the solve runs its iterations on the
- * split-precision matvec until the residual reaches tol or stops improving,
- * then continues from that vector with FP64 matvecs (defect correction) until
- * the FP64 residual reaches tol, so energy and residual are FP64 quantities.  `result`
+ * split-precision matvec until the residual reaches tol or, once below
+ * 1e-4 * max(1, |energy|), stops improving; then it continues from that
+ * vector with FP64 matvecs (defect correction) until the FP64 residual
+ * reaches tol, so energy and residual are FP64 quantities.  `result`
  * holds the initial guess and receives the normalised eigenvector; `energy`
  * receives the Ritz value.  Returns 0 when converged, 1 when max_its was
  * reached, T3NS_E* on failure.  `info` may be NULL. */
@@ -274,6 +275,41 @@ int t3ns_gesdd_host(char jobz, int m, int n, const double *a, int lda, double *s
                     int ldu, double *vt, int ldvt);
 int t3ns_geqrf_host(int m, int n, double *a, int lda, double *tau);
 int t3ns_orgqr_host(int m, int n, int k, double *a, int lda, const double *tau);
+
+/* Request loop for independent ground-state solves (no counterpart in the
+ * reference, whose driver runs one solve per process).  A request is one
+ * Davidson solve of an effective Hamiltonian, with the arguments of
+ * t3ns_davidson_host.  Requests are admitted in arrival order against a
+ * fixed device-memory budget (the first queued request that fits what the
+ * running ones leave free); up to max_inflight run at once, each on its own
+ * stream, so their work overlaps on the GPU.  A request whose estimated
+ * footprint exceeds the whole budget is rejected by submit (T3NS_E_LIMIT).
+ * The descriptor, guess/result and diagonal must stay valid until the
+ * request has been waited for; the result is written into guess_and_result. */
+typedef struct t3ns_server t3ns_server;
+typedef struct {
+        int64_t id;
+        int status;              /* the solve's return code (0, 1 or T3NS_E_*) */
+        double energy;
+        t3ns_davidson_info info;
+        int64_t bytes;           /* admitted footprint (estimate)             */
+        double queue_seconds;    /* submit -> admission                       */
+        double run_seconds;      /* admission -> result                       */
+        double latency_seconds;  /* submit -> result                          */
+} t3ns_request_result;
+
+int t3ns_server_create(int64_t budget_bytes, int max_inflight, t3ns_server **out);
+int t3ns_server_submit(t3ns_server *s, const t3ns_heff_desc *desc, int precision,
+                       double *guess_and_result, const double *diagonal, double tol, int max_its,
+                       int max_vecs, int keep, int64_t *id_out);
+/* Blocks until request `id` has finished; returns its status. */
+int t3ns_server_wait(t3ns_server *s, int64_t id, t3ns_request_result *out);
+/* Device bytes admitted now, the peak so far, and requests waiting. */
+int t3ns_server_stats(t3ns_server *s, int64_t *in_use, int64_t *peak, int *queued);
+/* Finishes queued and running requests, then frees the server. */
+void t3ns_server_destroy(t3ns_server *s);
+/* The footprint estimate admission uses (host only, no GPU needed). */
+int64_t t3ns_server_estimate_bytes(const t3ns_heff_desc *desc, int precision, int max_vecs);
 
 /* Largest vector t3ns_precondition_device_noalloc accepts (elements). */
 #define T3NS_NOALLOC_MAX_SIZE 16777216LL

@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 ENGINE_SOURCES = ["capi.cu", "heff.cu", "davidson.cu", "precond_noalloc.cu", "rops_update.cu",
-                  "dense.cu"]
+                  "dense.cu", "server.cu"]
 
 
 def _run(cmd, cwd=None):

@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <cmath>
 #include <functional>
 #include <string>
@@ -38,6 +39,7 @@ static constexpr int kRedThreads = 256;
 static constexpr int kChunk = 8;         // basis columns per register pass
 static constexpr double kDiagCutoff = 1e-12;
 static constexpr int kMaxVecs = 32;      // largest Davidson subspace
+static constexpr double kStallLevel = 1e-4;   // see davidson_core's `stall`
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -451,9 +453,10 @@ static int alloc_basis(DavidsonBuffers &b, int64_t n, int max_vecs)
 // y = H x on device vectors, enqueued on the given stream
 using DevMatvec = std::function<int(const double *, double *, cudaStream_t)>;
 
-// stall > 0: also stop (returning 2) once the residual has not fallen below
-// 0.9 of its best value for `stall` iterations (the split-precision phase,
-// whose residual levels off at the matvec's rounding).
+// stall > 0: also stop (returning 2) once the residual is below
+// kStallLevel * max(1, |energy|) -- the region where the split-precision
+// matvec's rounding (~2e-6 relative) can level it off -- and has not fallen
+// below 0.9 of its best value for `stall` iterations.
 static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, double *energy,
                          int max_vecs, int keep, double tol, int max_its, const double *d_diag,
                          t3ns_davidson_info *info, cudaStream_t s, int stall = 0,
@@ -592,7 +595,8 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                 if (its == 0 || res < 0.9 * best_res) {
                         best_res = res;
                         since_best = 0;
-                } else if (stall > 0 && ++since_best >= stall) {
+                } else if (stall > 0 && ++since_best >= stall &&
+                           res < kStallLevel * std::max(1.0, fabs(b.host_scal[3]))) {
                         stalled = true;
                 }
                 const double theta = b.host_scal[3];

@@ -927,7 +927,9 @@ static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const T *x, c
                                                    (int) smem_bytes_t<Cfg, T>()));
                 attr_set = true;
         }
-        heff_kernel<Cfg, T><<<dt.grid, Cfg::kThreads, smem_bytes_t<Cfg, T>(), s>>>(
+        const int share = dp.share ? std::max(1, dp.share->load(std::memory_order_relaxed)) : 1;
+        const int grid = std::max(1, dt.grid / share);
+        heff_kernel<Cfg, T><<<grid, Cfg::kThreads, smem_bytes_t<Cfg, T>(), s>>>(
                 x, y, ops, dp.blk_off, dp.edims, dt.units, dt.n_units, dt.pair_ptr, dt.pairs,
                 dp.tasks, dp.counter, dp.err);
         T3NS_CUDA_TRY(cudaGetLastError());

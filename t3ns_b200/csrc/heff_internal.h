@@ -1,6 +1,7 @@
 // Internal data structures of the matvec engine (host plan, device plan).
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <vector>
 
@@ -109,6 +110,10 @@ struct DevicePlan {
         HeffTask *tasks = nullptr;
         DeviceTiles tiles[kNumCfgs];
         int active = 0;                           // configuration the matvec runs
+        // when set (by the request loop), the number of solves sharing the
+        // GPU: each matvec launch takes that share of the persistent grid, so
+        // concurrent solves run side by side instead of queueing for SMs
+        const std::atomic<int> *share = nullptr;
         int *counter = nullptr;                   // dynamic unit scheduler
         int *err = nullptr;
 };

@@ -65,6 +65,12 @@ class DavidsonInfo(C.Structure):
                 ("residual", C.c_double), ("seconds", C.c_double), ("fp64_iterations", C.c_int)]
 
 
+class RequestResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int), ("energy", C.c_double),
+                ("info", DavidsonInfo), ("bytes", C.c_int64), ("queue_seconds", C.c_double),
+                ("run_seconds", C.c_double), ("latency_seconds", C.c_double)]
+
+
 _lib = None
 
 
@@ -99,6 +105,17 @@ def load(path: str | None = None):
                                              C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                                              C.c_void_p]
     lib.t3ns_precondition_host.argtypes = [C.c_int64, _f64p, C.c_double, _f64p, _f64p]
+    lib.t3ns_server_create.argtypes = [C.c_int64, C.c_int, C.POINTER(C.c_void_p)]
+    lib.t3ns_server_submit.argtypes = [C.c_void_p, C.POINTER(HeffDesc), C.c_int, _f64p, _f64p,
+                                       C.c_double, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_int64)]
+    lib.t3ns_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(RequestResult)]
+    lib.t3ns_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int)]
+    lib.t3ns_server_destroy.argtypes = [C.c_void_p]
+    lib.t3ns_server_destroy.restype = None
+    lib.t3ns_server_estimate_bytes.argtypes = [C.POINTER(HeffDesc), C.c_int, C.c_int]
+    lib.t3ns_server_estimate_bytes.restype = C.c_int64
     lib.t3ns_precondition_device_noalloc.argtypes = [C.c_int64, C.c_void_p, C.c_double,
                                                      C.c_void_p, C.c_void_p, C.c_void_p]
     if path is None:
