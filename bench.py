@@ -311,7 +311,7 @@ def davidson_comparison(path=None, max_its=100, seed=7):
     them) to tol 1e-5, with FP64 matvecs and with split-precision matvecs
     plus FP64 defect correction: seconds, iterations and the energy
     difference.  The guess stands in for the previous step's state the sweep
-    would pass: an untimed FP64 solve to 1e-3 from a seeded random vector.
+    would pass: an untimed FP64 solve to 3e-3 from a seeded random vector.
     None if the step is not present."""
     path = path or os.path.join(ROOT, "oracle", "_ref", "captures", "qc24_D512", "step_006.t3c")
     if not os.path.exists(path):
@@ -323,10 +323,12 @@ def davidson_comparison(path=None, max_its=100, seed=7):
     g0 = np.random.default_rng(seed).standard_normal(s["diag"].size)
     g0 /= np.linalg.norm(g0)
     pre = HeffPlan(desc)
-    pre.davidson_host(g0, s["diag"], tol=1e-3, max_its=300)
+    _, _, pinfo = pre.davidson_host(g0, s["diag"], tol=3e-3, max_its=200)
     pre.close()
     out = {"step": os.path.relpath(path, ROOT), "psi_elems": int(s["diag"].size), "tol": 1e-5,
-           "max_its": max_its, "guess": "FP64 solve to 1e-3 from seeded N(0,1)"}
+           "max_its": max_its,
+           "guess": "FP64 solve from seeded N(0,1) to residual %.1e (%d iterations)"
+                    % (pinfo["residual"], pinfo["iterations"])}
     for name, prec in (("fp64", T3NS_PREC_FP64), ("3xtf32", T3NS_PREC_3XTF32)):
         plan = HeffPlan(desc, prec)
         plan.autotune(reps=1, force=False)
