@@ -80,10 +80,12 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 }
 
 // Warp tile of (8*RM) x (8*RN) outputs: RM*RN mma per k-step sharing RM A
-// fragments and RN B fragments, B(k, n) = Bb[k*bk + n*bn]; the next k-step's
-// fragments are loaded before the current step's mma are issued.  Loop
-// bounds are warp-uniform (mma.sync needs the whole warp); lanes outside
-// M, N or K load zeros.
+// fragments and RN B fragments, A(m, k) = Ab[m + k*ak], B(k, n) =
+// Bb[k*bk + n*bn]; the next k-step's fragments are loaded before the current
+// step's mma are issued.  The K loop runs its full 4-wide steps on pointers
+// advanced in place (no per-element index arithmetic or K bound) and a
+// predicated tail step.  Loop bounds are warp-uniform (mma.sync needs the
+// whole warp); lanes outside M or N read row / column 0 and use zeros.
 template <int RM, int RN>
 __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const double *Ab, int ak,
                                               const double *Bb, int bk, int bn, int K, int M,
@@ -95,36 +97,72 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
         for (int i = 0; i < RM; ++i) {
                 const int m = m0 + 8 * i + lr;
                 mok[i] = m < M;
-                ap[i] = Ab + (mok[i] ? m : 0);
+                ap[i] = Ab + (mok[i] ? m : 0) + (int64_t) lc * ak;
         }
 #pragma unroll
         for (int j = 0; j < RN; ++j) {
                 const int n = n0 + 8 * j + lr;
                 nok[j] = n < N;
-                bp[j] = Bb + (nok[j] ? n : 0) * bn;
+                bp[j] = Bb + (int64_t) (nok[j] ? n : 0) * bn + (int64_t) lc * bk;
         }
+        const int64_t astep = 4 * (int64_t) ak, bstep = 4 * (int64_t) bk;
+        const int full = K >> 2;
         double a[RM], b[RN];
-        auto load = [&](int k0) {
-                const int k = k0 + lc;
-                const bool kok = k < K;
+        auto load_step = [&]() {
 #pragma unroll
-                for (int i = 0; i < RM; ++i) a[i] = (mok[i] && kok) ? ap[i][k * ak] : 0.0;
+                for (int i = 0; i < RM; ++i) {
+                        a[i] = mok[i] ? *ap[i] : 0.0;
+                        ap[i] += astep;
+                }
 #pragma unroll
-                for (int j = 0; j < RN; ++j) b[j] = (nok[j] && kok) ? bp[j][k * bk] : 0.0;
+                for (int j = 0; j < RN; ++j) {
+                        b[j] = nok[j] ? *bp[j] : 0.0;
+                        bp[j] += bstep;
+                }
         };
-        load(0);
-        for (int k0 = 0; k0 < K; k0 += 4) {
-                double ca[RM], cb[RN];
+        if (full > 0) {
+                load_step();
+                for (int st = 0; st < full; ++st) {
+                        double ca[RM], cb[RN];
 #pragma unroll
-                for (int i = 0; i < RM; ++i) ca[i] = a[i];
+                        for (int i = 0; i < RM; ++i) ca[i] = a[i];
 #pragma unroll
-                for (int j = 0; j < RN; ++j) cb[j] = b[j];
-                if (k0 + 4 < K) load(k0 + 4);
+                        for (int j = 0; j < RN; ++j) cb[j] = b[j];
+                        if (st + 1 < full) load_step();
+#pragma unroll
+                        for (int i = 0; i < RM; ++i)
+#pragma unroll
+                                for (int j = 0; j < RN; ++j)
+                                        dmma_8x8x4(d[i][j][0], d[i][j][1], ca[i], cb[j]);
+                }
+        }
+        if (K & 3) {
+                const bool kok = lc < (K & 3);
+#pragma unroll
+                for (int i = 0; i < RM; ++i) a[i] = (mok[i] && kok) ? *ap[i] : 0.0;
+#pragma unroll
+                for (int j = 0; j < RN; ++j) b[j] = (nok[j] && kok) ? *bp[j] : 0.0;
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
-                        for (int j = 0; j < RN; ++j) dmma_8x8x4(d[i][j][0], d[i][j][1], ca[i], cb[j]);
+                        for (int j = 0; j < RN; ++j) dmma_8x8x4(d[i][j][0], d[i][j][1], a[i], b[j]);
         }
+}
+
+// q = a / b, r = a % b for 0 <= a < 2^22 and b > 0, with rb = 1.0f / b: the
+// float quotient is off by at most one, which one correction step fixes.
+__device__ __forceinline__ int fast_divmod(int a, int b, float rb, int &r)
+{
+        int q = __float2int_rz(__int2float_rz(a) * rb);
+        r = a - q * b;
+        if (r < 0) {
+                --q;
+                r += b;
+        } else if (r >= b) {
+                ++q;
+                r -= b;
+        }
+        return q;
 }
 
 // One contraction stage for G terms.  Term g applies rows [row0, row0+rows)
@@ -159,12 +197,14 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
         const int items = (ACC ? 1 : G) * nc * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int lr = lane >> 2, lc = lane & 3;
+        const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt, r_nc = 1.0f / nc;
         for (int it = warp; it < items; it += NW) {
-                const int tile = it % tiles;
-                const int gc = it / tiles;
-                const int tm = tile % mt, tn = tile / mt;
-                const int c = ACC ? gc : gc % nc;
-                const int g0 = ACC ? 0 : gc / nc;
+                int tile, tm, cc;
+                const int gc = fast_divmod(it, tiles, r_tiles, tile);
+                const int tn = fast_divmod(tile, mt, r_mt, tm);
+                const int gq = fast_divmod(gc, nc, r_nc, cc);
+                const int c = ACC ? gc : cc;
+                const int g0 = ACC ? 0 : gq;
                 const int g1 = ACC ? G : g0 + 1;
                 const int m0 = tm * 8 * RM, n0 = tn * 8 * RN;
                 double d[RM][RN][2];
@@ -319,12 +359,14 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
         const int items = (ACC ? 1 : G) * nc * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int g = lane >> 2, t = lane & 3;
+        const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt, r_nc = 1.0f / nc;
         for (int it = warp; it < items; it += NW) {
-                const int tile = it % tiles;
-                const int gc = it / tiles;
-                const int tm = tile % mt, tn = tile / mt;
-                const int c = ACC ? gc : gc % nc;
-                const int g0 = ACC ? 0 : gc / nc;
+                int tile, tm, cc;
+                const int gc = fast_divmod(it, tiles, r_tiles, tile);
+                const int tn = fast_divmod(tile, mt, r_mt, tm);
+                const int gq = fast_divmod(gc, nc, r_nc, cc);
+                const int c = ACC ? gc : cc;
+                const int g0 = ACC ? 0 : gq;
                 const int g1 = ACC ? G : g0 + 1;
                 const int m0 = tm * 16 * RM, n0 = tn * 8 * RN;
                 float d[RM][RN][4];
