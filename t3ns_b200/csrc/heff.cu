@@ -79,6 +79,45 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
                      : "d"(a), "d"(b));
 }
 
+// q = a / b, r = a % b for 0 <= a < 2^22 and b > 0, with rb = 1.0f / b: the
+// float quotient is off by at most one, which one correction step fixes.
+__device__ __forceinline__ int fast_divmod(int a, int b, float rb, int &r)
+{
+        int q = __float2int_rz(__int2float_rz(a) * rb);
+        r = a - q * b;
+        if (r < 0) {
+                --q;
+                r += b;
+        } else if (r >= b) {
+                ++q;
+                r -= b;
+        }
+        return q;
+}
+
+// GEMM row m of a stage -> element offset of its row in A and in C.  A stage
+// on memory axis 1 runs its w[2] slices as one GEMM with M = w[0] * w[2]
+// (row m = slice m / w[0], row m % w[0] of the slice), so a small w[0] is
+// padded once instead of per slice; the other stages have plain rows.
+struct RowSplit {
+        int div;          // rows per slice (1 << 30 when unsplit)
+        float rdiv;
+        int64_t a_slice;  // slice stride in A
+        int64_t c_slice;  // slice stride in C
+        __device__ __forceinline__ int64_t a_off(int m) const
+        {
+                int r;
+                const int q = fast_divmod(m, div, rdiv, r);
+                return r + q * a_slice;
+        }
+        __device__ __forceinline__ int64_t c_off(int m) const
+        {
+                int r;
+                const int q = fast_divmod(m, div, rdiv, r);
+                return r + q * c_slice;
+        }
+};
+
 // Warp tile of (8*RM) x (8*RN) outputs: RM*RN mma per k-step sharing RM A
 // fragments and RN B fragments, A(m, k) = Ab[m + k*ak], B(k, n) =
 // Bb[k*bk + n*bn]; the next k-step's fragments are loaded before the current
@@ -88,8 +127,9 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 // whole warp); lanes outside M or N read row / column 0 and use zeros.
 template <int RM, int RN>
 __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const double *Ab, int ak,
-                                              const double *Bb, int bk, int bn, int K, int M,
-                                              int N, int m0, int n0, int lr, int lc)
+                                              const RowSplit &rs, const double *Bb, int bk,
+                                              int bn, int K, int M, int N, int m0, int n0, int lr,
+                                              int lc)
 {
         bool mok[RM], nok[RN];
         const double *ap[RM], *bp[RN];
@@ -97,7 +137,7 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
         for (int i = 0; i < RM; ++i) {
                 const int m = m0 + 8 * i + lr;
                 mok[i] = m < M;
-                ap[i] = Ab + (mok[i] ? m : 0) + (int64_t) lc * ak;
+                ap[i] = Ab + rs.a_off(mok[i] ? m : 0) + (int64_t) lc * ak;
         }
 #pragma unroll
         for (int j = 0; j < RN; ++j) {
@@ -149,22 +189,6 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
         }
 }
 
-// q = a / b, r = a % b for 0 <= a < 2^22 and b > 0, with rb = 1.0f / b: the
-// float quotient is off by at most one, which one correction step fixes.
-__device__ __forceinline__ int fast_divmod(int a, int b, float rb, int &r)
-{
-        int q = __float2int_rz(__int2float_rz(a) * rb);
-        r = a - q * b;
-        if (r < 0) {
-                --q;
-                r += b;
-        } else if (r >= b) {
-                ++q;
-                r -= b;
-        }
-        return q;
-}
-
 // One contraction stage for G terms.  Term g applies rows [row0, row0+rows)
 // of the operator block at ops + opoff[g] (leading dimension ldop) on axis ax
 // of `in + g * in_gs` (dims w), writing `out + g * out_gs` (scaled by
@@ -179,32 +203,32 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
                                                 int in_gs, double *out, int out_gs,
                                                 const double *scale)
 {
-        int M, N, K, nc, ak, bk, bn, cn, a_cs, c_cs;
-        // A(m,k) = Ab[m + k*ak], B(k,n) = Bb[k*bk + n*bn], C(m,n) = Cb[m + n*cn]
+        int M, N, K, ak, bk, bn, cn;
+        RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
+        // A(m,k) = Ab[rs.a_off(m) + k*ak], B(k,n) = Bb[k*bk + n*bn],
+        // C(m,n) = Cb[rs.c_off(m) + n*cn]
         if (ax == 0) {
-                M = rows; N = w[1] * w[2]; K = w[0]; nc = 1;
-                ak = ldop; bk = 1; bn = K; cn = rows; a_cs = 0; c_cs = 0;
+                M = rows; N = w[1] * w[2]; K = w[0];
+                ak = ldop; bk = 1; bn = K; cn = rows;
         } else if (ax == 1) {
-                M = w[0]; N = rows; K = w[1]; nc = w[2];
+                M = w[0] * w[2]; N = rows; K = w[1];
                 ak = w[0]; bk = ldop; bn = 1; cn = w[0];
-                a_cs = w[0] * w[1]; c_cs = w[0] * rows;
+                rs = RowSplit{w[0], 1.0f / w[0], (int64_t) w[0] * w[1], (int64_t) w[0] * rows};
         } else {
-                M = w[0] * w[1]; N = rows; K = w[2]; nc = 1;
-                ak = M; bk = ldop; bn = 1; cn = M; a_cs = 0; c_cs = 0;
+                M = w[0] * w[1]; N = rows; K = w[2];
+                ak = M; bk = ldop; bn = 1; cn = M;
         }
         const int mt = (M + 8 * RM - 1) / (8 * RM), nt = (N + 8 * RN - 1) / (8 * RN);
         const int tiles = mt * nt;
-        const int items = (ACC ? 1 : G) * nc * tiles;
+        const int items = (ACC ? 1 : G) * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int lr = lane >> 2, lc = lane & 3;
-        const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt, r_nc = 1.0f / nc;
+        const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt;
         for (int it = warp; it < items; it += NW) {
-                int tile, tm, cc;
-                const int gc = fast_divmod(it, tiles, r_tiles, tile);
+                int tile, tm;
+                const int g0 = ACC ? 0 : fast_divmod(it, tiles, r_tiles, tile);
+                if (ACC) tile = it;
                 const int tn = fast_divmod(tile, mt, r_mt, tm);
-                const int gq = fast_divmod(gc, nc, r_nc, cc);
-                const int c = ACC ? gc : cc;
-                const int g0 = ACC ? 0 : gq;
                 const int g1 = ACC ? G : g0 + 1;
                 const int m0 = tm * 8 * RM, n0 = tn * 8 * RN;
                 double d[RM][RN][2];
@@ -215,23 +239,24 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
                 for (int g = g0; g < g1; ++g) {
                         const double *op = ops + opoff[g];
                         const double *tin = in + g * in_gs;
-                        const double *Ab = ax == 0 ? op : tin + c * a_cs;
+                        const double *Ab = ax == 0 ? op : tin;
                         const double *Bb = ax == 0 ? tin : op;
-                        warp_tile_mma<RM, RN>(d, Ab, ak, Bb, bk, bn, K, M, N, m0, n0, lr, lc);
+                        warp_tile_mma<RM, RN>(d, Ab, ak, rs, Bb, bk, bn, K, M, N, m0, n0, lr, lc);
                 }
                 const double sc = (!ACC && scale) ? scale[g0] : 1.0;
-                double *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs;
+                double *Cb = out + (ACC ? 0 : g0 * out_gs);
 #pragma unroll
                 for (int i = 0; i < RM; ++i) {
                         const int mc = m0 + 8 * i + lr;
                         if (mc >= M) continue;
+                        double *crow = Cb + rs.c_off(mc);
 #pragma unroll
                         for (int j = 0; j < RN; ++j) {
                                 const int nc0 = n0 + 8 * j + 2 * lc;
 #pragma unroll
                                 for (int h = 0; h < 2; ++h) {
                                         if (nc0 + h >= N) continue;
-                                        double *cp = Cb + mc + (nc0 + h) * cn;
+                                        double *cp = crow + (nc0 + h) * cn;
                                         *cp = ACC ? *cp + d[i][j][h] : sc * d[i][j][h];
                                 }
                         }
@@ -248,7 +273,7 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                                               int in_gs, double *out, int out_gs,
                                               const double *scale)
 {
-        const int M = ax == 0 ? rows : ax == 1 ? w[0] : w[0] * w[1];
+        const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
         if (M <= 8)
                 grouped_stage_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
@@ -288,14 +313,35 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
                      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Warp tile of (16*RM) x (8*RN) outputs, A(m,k) = Ab[m*am + k*ak],
-// B(k,n) = Bb[k*bk + n*bn]; loop bounds warp-uniform, lanes outside M, N or K
-// load zeros.
+// Warp tile of (16*RM) x (8*RN) outputs.  A(m,k) = Ab[arow(m) + k*ak] and
+// B(k,n) = Bb[k*bk + bcol(n)], where the row (column) offsets are the
+// stage's RowSplit offsets on the split side (split_a: rows of A, else
+// columns of B) and m*am (n*bn) otherwise; offsets are taken once per tile.
+// Loop bounds warp-uniform; lanes outside M, N or K load zeros.
 template <int RM, int RN>
 __device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const float *Ab, int am,
-                                                 int ak, const float *Bb, int bk, int bn, int K,
-                                                 int M, int N, int m0, int n0, int g, int t)
+                                                 int ak, const float *Bb, int bk, int bn,
+                                                 const RowSplit &rs, bool split_a, int K, int M,
+                                                 int N, int m0, int n0, int g, int t)
 {
+        int64_t arow[RM][2], bcol[RN];
+        bool mok[RM][2], nok[RN];
+#pragma unroll
+        for (int i = 0; i < RM; ++i)
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                        const int m = m0 + 16 * i + 8 * r + g;
+                        mok[i][r] = m < M;
+                        const int mm = mok[i][r] ? m : 0;
+                        arow[i][r] = split_a ? rs.a_off(mm) : (int64_t) mm * am;
+                }
+#pragma unroll
+        for (int j = 0; j < RN; ++j) {
+                const int n = n0 + 8 * j + g;
+                nok[j] = n < N;
+                const int nn = nok[j] ? n : 0;
+                bcol[j] = split_a ? (int64_t) nn * bn : rs.a_off(nn);
+        }
         for (int k0 = 0; k0 < K; k0 += 8) {
                 const int kk[2] = {k0 + t, k0 + t + 4};
                 uint32_t ah[RM][4], al[RM][4], bh[RN][2], bl[RN][2];
@@ -305,19 +351,20 @@ __device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const fl
                         for (int c = 0; c < 2; ++c)
 #pragma unroll
                                 for (int r = 0; r < 2; ++r) {
-                                        const int m = m0 + 16 * i + 8 * r + g;
-                                        const float v = (m < M && kk[c] < K) ? Ab[m * am + kk[c] * ak] : 0.f;
+                                        const float v = (mok[i][r] && kk[c] < K)
+                                                                ? Ab[arow[i][r] + (int64_t) kk[c] * ak]
+                                                                : 0.f;
                                         split_tf32(v, ah[i][r + 2 * c], al[i][r + 2 * c]);
                                 }
 #pragma unroll
-                for (int j = 0; j < RN; ++j) {
-                        const int n = n0 + 8 * j + g;
+                for (int j = 0; j < RN; ++j)
 #pragma unroll
                         for (int c = 0; c < 2; ++c) {
-                                const float v = (n < N && kk[c] < K) ? Bb[kk[c] * bk + n * bn] : 0.f;
+                                const float v = (nok[j] && kk[c] < K)
+                                                        ? Bb[(int64_t) kk[c] * bk + bcol[j]]
+                                                        : 0.f;
                                 split_tf32(v, bh[j][c], bl[j][c]);
                         }
-                }
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -338,35 +385,35 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
                                                     const float *in, int in_gs, float *out,
                                                     int out_gs, const float *scale, bool swap)
 {
-        int M, N, K, nc, ak, bk, bn, cn, a_cs, c_cs;
+        int M, N, K, ak, bk, bn, cn;
+        RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
+        // A(m,k) = Ab[rs.a_off(m) + k*ak], B(k,n) = Bb[k*bk + n*bn],
+        // C(m,n) = Cb[rs.c_off(m) + n*cn]  (axis 1: slices merged into M)
         if (ax == 0) {
-                M = rows; N = w[1] * w[2]; K = w[0]; nc = 1;
-                ak = ldop; bk = 1; bn = K; cn = rows; a_cs = 0; c_cs = 0;
+                M = rows; N = w[1] * w[2]; K = w[0];
+                ak = ldop; bk = 1; bn = K; cn = rows;
         } else if (ax == 1) {
-                M = w[0]; N = rows; K = w[1]; nc = w[2];
+                M = w[0] * w[2]; N = rows; K = w[1];
                 ak = w[0]; bk = ldop; bn = 1; cn = w[0];
-                a_cs = w[0] * w[1]; c_cs = w[0] * rows;
+                rs = RowSplit{w[0], 1.0f / w[0], (int64_t) w[0] * w[1], (int64_t) w[0] * rows};
         } else {
-                M = w[0] * w[1]; N = rows; K = w[2]; nc = 1;
-                ak = M; bk = ldop; bn = 1; cn = M; a_cs = 0; c_cs = 0;
+                M = w[0] * w[1]; N = rows; K = w[2];
+                ak = M; bk = ldop; bn = 1; cn = M;
         }
-        // tile orientation: (M', N') with A'(m',k) and B'(k,n'), C'(m',n') = C[m'*cm + n'*cnn]
+        // tile orientation (M', N'): swapped, A'(m', k) = B(k, m') and
+        // B'(k, n') = A(n', k), whose split rows become B' columns
         const int Mt = swap ? N : M, Nt = swap ? M : N;
-        const int am = swap ? bn : 1, akk = swap ? bk : ak, bkk = swap ? ak : bk, bnn = swap ? 1 : bn;
-        const int cm = swap ? cn : 1, cnn = swap ? 1 : cn;
         const int mt = (Mt + 16 * RM - 1) / (16 * RM), nt = (Nt + 8 * RN - 1) / (8 * RN);
         const int tiles = mt * nt;
-        const int items = (ACC ? 1 : G) * nc * tiles;
+        const int items = (ACC ? 1 : G) * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int g = lane >> 2, t = lane & 3;
-        const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt, r_nc = 1.0f / nc;
+        const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt;
         for (int it = warp; it < items; it += NW) {
-                int tile, tm, cc;
-                const int gc = fast_divmod(it, tiles, r_tiles, tile);
+                int tile, tm;
+                const int g0 = ACC ? 0 : fast_divmod(it, tiles, r_tiles, tile);
+                if (ACC) tile = it;
                 const int tn = fast_divmod(tile, mt, r_mt, tm);
-                const int gq = fast_divmod(gc, nc, r_nc, cc);
-                const int c = ACC ? gc : cc;
-                const int g0 = ACC ? 0 : gq;
                 const int g1 = ACC ? G : g0 + 1;
                 const int m0 = tm * 16 * RM, n0 = tn * 8 * RN;
                 float d[RM][RN][4];
@@ -379,13 +426,17 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
                 for (int gg = g0; gg < g1; ++gg) {
                         const float *op = ops + opoff[gg];
                         const float *tin = in + gg * in_gs;
-                        const float *Ab = ax == 0 ? op : tin + c * a_cs;
+                        const float *Ab = ax == 0 ? op : tin;
                         const float *Bb = ax == 0 ? tin : op;
-                        warp_tile_tf32x3<RM, RN>(d, swap ? Bb : Ab, am, akk, swap ? Ab : Bb, bkk, bnn, K,
-                                                 Mt, Nt, m0, n0, g, t);
+                        if (swap)
+                                warp_tile_tf32x3<RM, RN>(d, Bb, bn, bk, Ab, ak, 1, rs, false, K, Mt, Nt,
+                                                         m0, n0, g, t);
+                        else
+                                warp_tile_tf32x3<RM, RN>(d, Ab, 1, ak, Bb, bk, bn, rs, true, K, Mt, Nt,
+                                                         m0, n0, g, t);
                 }
                 const float sc = (!ACC && scale) ? scale[g0] : 1.f;
-                float *Cb = out + (ACC ? 0 : g0 * out_gs) + c * c_cs;
+                float *Cb = out + (ACC ? 0 : g0 * out_gs);
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -398,7 +449,9 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
                                         for (int h = 0; h < 2; ++h) {
                                                 const int ncol = n0 + 8 * j + 2 * t + h;
                                                 if (ncol >= Nt) continue;
-                                                float *cp = Cb + mc * cm + ncol * cnn;
+                                                // C(m, n) with (m, n) = swap ? (ncol, mc) : (mc, ncol)
+                                                float *cp = swap ? Cb + rs.c_off(ncol) + (int64_t) mc * cn
+                                                                 : Cb + rs.c_off(mc) + (int64_t) ncol * cn;
                                                 const float v = d[i][j][2 * r + h];
                                                 *cp = ACC ? *cp + v : sc * v;
                                         }
@@ -412,7 +465,7 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                                               const float *in, int in_gs, float *out, int out_gs,
                                               const float *scale)
 {
-        const int M = ax == 0 ? rows : ax == 1 ? w[0] : w[0] * w[1];
+        const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
         // padded work of the two orientations (16 x 8 granules)
         const int64_t pw0 = (int64_t) ((M + 15) / 16) * ((N + 7) / 8);
@@ -623,28 +676,64 @@ static double seq_cost(const int *seq, int nst, const int *o, const int *n, cons
         return fl;
 }
 
-// Cheapest contraction sequence for a pair on a tiling (ext, nt) among those
-// whose intermediates fit the shared buffer.  Returns -1 if none fits.
+// Tensor-pipe work of the same sequence: each stage as the kernel maps it
+// to GEMMs (axis 0: M = rows, N = the other two dims; axis 1: M = dims 0
+// and 2, N = rows; axis 2: M = dims 0 and 1, N = rows; K = the old dim),
+// with M and N padded to the 8 of an mma.m8n8k4 tile and K to its 4, per
+// tile (extent ext) times the number of tiles.  Thin tiles and small dims
+// cost what they occupy on the pipe, not their FLOPs.
+static double tile_cost(const int *seq, int nst, const int *o, const int *ext, const int *nt)
+{
+        auto p8 = [](int64_t x) { return (double) ((x + 7) / 8 * 8); };
+        auto p4 = [](int64_t x) { return (double) ((x + 3) / 4 * 4); };
+        int64_t cur[3] = {o[0], o[1], o[2]};
+        double c = 0;
+        for (int s = 0; s < nst; ++s) {
+                const int a = seq[s];
+                const int64_t rows = ext[a];
+                double m, n;
+                if (a == 0) {
+                        m = p8(rows);
+                        n = p8(cur[1] * cur[2]);
+                } else if (a == 1) {
+                        m = p8(cur[0] * cur[2]);
+                        n = p8(rows);
+                } else {
+                        m = p8(cur[0] * cur[1]);
+                        n = p8(rows);
+                }
+                c += 2.0 * m * n * p4(cur[a]);
+                cur[a] = rows;
+        }
+        return c * nt[0] * nt[1] * nt[2];
+}
+
+// Cheapest contraction sequence for a pair on a tiling (ext, nt) by
+// tensor-pipe work, among those whose intermediates fit the shared buffer;
+// fl_out receives its FLOPs and pc_out its tensor-pipe work.  Returns -1 if
+// none fits.
 static int choose_seq(int nst, const int *o, const int *n, const int *ext, const int *nt,
-                      int w_cap, double *fl_out, int seq_out[3])
+                      int w_cap, double *fl_out, double *pc_out, int seq_out[3])
 {
         static const int perms3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
                                          {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
         static const int perms2[2][3] = {{0, 1, 2}, {1, 0, 2}};
         const int np = nst == 3 ? 6 : 2;
         int best = -1;
-        double bfl = 0;
+        double bfl = 0, bpc = 0;
         for (int q = 0; q < np; ++q) {
                 const int *seq = nst == 3 ? perms3[q] : perms2[q];
                 int64_t s1 = 0, s2 = 0;
                 const double fl = seq_cost(seq, nst, o, n, ext, nt, &s1, &s2);
                 if (s1 + s2 > w_cap) continue;
-                if (best < 0 || fl < bfl) { best = q; bfl = fl; }
+                const double pc = tile_cost(seq, nst, o, ext, nt);
+                if (best < 0 || pc < bpc) { best = q; bfl = fl; bpc = pc; }
         }
         if (best < 0) return -1;
         const int *seq = nst == 3 ? perms3[best] : perms2[best];
         for (int s = 0; s < 3; ++s) seq_out[s] = seq[s];
         *fl_out = bfl;
+        *pc_out = bpc;
         return 0;
 }
 
@@ -854,12 +943,12 @@ int tile_plan(HostPlan &hp, int cfg)
                         const int nt[3] = {(en[0] + cd.at - 1) / cd.at, (en[1] + cd.bt - 1) / cd.bt,
                                            (en[2] + cd.ct - 1) / cd.ct};
                         std::vector<int> seqs(ptmp.size());
-                        double fl_blk = 0;
+                        double fl_blk = 0, pc_blk = 0;
                         bool ok = true;
                         for (size_t q = 0; q < ptmp.size() && ok; ++q) {
                                 int seq[3];
-                                double fl;
-                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, kc.w_cap, &fl, seq) != 0) {
+                                double fl, pc;
+                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, kc.w_cap, &fl, &pc, seq) != 0) {
                                         ok = false;
                                         break;
                                 }
@@ -867,15 +956,16 @@ int tile_plan(HostPlan &hp, int cfg)
                                 for (int st = 0; st < nops; ++st) axes |= seq[st] << (2 * st);
                                 seqs[q] = axes;
                                 fl_blk += fl * (ptmp[q].t1 - ptmp[q].t0);
+                                pc_blk += pc * (ptmp[q].t1 - ptmp[q].t0);
                         }
                         if (!ok) continue;
-                        // cost: FLOPs plus a fixed charge per (unit, pair) visit
-                        // (staging the old block, group barriers), which keeps
-                        // tiles from shrinking for a marginal FLOP saving
+                        // cost: tensor-pipe work plus a fixed charge per (unit,
+                        // pair) visit (staging the old block, group barriers),
+                        // which keeps tiles from shrinking for a marginal saving
                         const double nunits = std::ceil((double) en[0] / cd.at) *
                                               std::ceil((double) en[1] / cd.bt) *
                                               std::ceil((double) en[2] / cd.ct);
-                        const double cost = fl_blk + kPairVisitCost * nunits * ptmp.size();
+                        const double cost = pc_blk + kPairVisitCost * nunits * ptmp.size();
                         if (best_ci < 0 || cost < best_cost) {
                                 best_ci = (int) ci;
                                 best_fl = fl_blk;
