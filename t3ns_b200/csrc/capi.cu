@@ -77,7 +77,8 @@ static int upload_tiles(t3ns_heff *h, int cfg)
         return T3NS_OK;
 }
 
-// FP32 operator copy and input staging of the split-precision matvec.
+// Pre-split {hi, lo} operator copy and input staging of the split-precision
+// matvec.
 static int setup_precision(t3ns_heff *h, int precision)
 {
         if (precision == T3NS_PREC_BF16X3)
@@ -86,10 +87,10 @@ static int setup_precision(t3ns_heff *h, int precision)
         if (precision != T3NS_PREC_FP64 && precision != T3NS_PREC_3XTF32)
                 return set_error(T3NS_E_ARG, "unknown precision");
         DevicePlan &dp = h->dp;
-        if (precision == T3NS_PREC_3XTF32 && !dp.ops32) {
-                T3NS_TRY(dev_alloc(h, &dp.ops32, (size_t) h->hp.op_elems));
-                T3NS_TRY(dev_alloc(h, &dp.x32, (size_t) h->hp.size));
-                T3NS_TRY(convert_to_f32(dp.ops, dp.ops32, h->hp.op_elems, h->stream));
+        if (precision == T3NS_PREC_3XTF32 && !dp.ops_split) {
+                T3NS_TRY(dev_alloc(h, &dp.ops_split, (size_t) h->hp.op_elems));
+                T3NS_TRY(dev_alloc(h, &dp.x_split, (size_t) h->hp.size));
+                T3NS_TRY(convert_to_split(dp.ops, dp.ops_split, h->hp.op_elems, h->stream));
                 T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
         }
         h->precision = precision;

@@ -284,10 +284,13 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
 }
 
 // ---------------------------------------------------------------------------
-// Split-precision stages: FP32 data, products on the TF32 tensor pipe
-// (mma.m16n8k8) as 3xTF32 -- x = hi + lo with hi = tf32(x), lo = tf32(x - hi),
+// Split-precision stages: products on the TF32 tensor pipe (mma.m16n8k8) as
+// 3xTF32 -- x = hi + lo with hi = tf32(x), lo = tf32(x - hi),
 // x*y ~ lo_x*hi_y + hi_x*lo_y + hi_x*hi_y (the lo*lo term, ~2^-22 relative,
-// is dropped) -- with FP32 accumulation.
+// is dropped) -- with FP32 accumulation.  Operands are stored already split,
+// as float2 {hi, lo}: the operators once per plan, Psi once per matvec, and
+// every intermediate when a stage writes it, so the inner loop loads a pair
+// and issues the three products with no conversion.
 
 __device__ __forceinline__ uint32_t to_tf32(float x)
 {
@@ -296,10 +299,10 @@ __device__ __forceinline__ uint32_t to_tf32(float x)
         return r;
 }
 
-__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo)
+__device__ __forceinline__ float2 split_tf32(float x)
 {
-        hi = to_tf32(x);
-        lo = to_tf32(x - __uint_as_float(hi));
+        const uint32_t hi = to_tf32(x);
+        return make_float2(__uint_as_float(hi), __uint_as_float(to_tf32(x - __uint_as_float(hi))));
 }
 
 // D(16x8) += A(16x8) * B(8x8).  Fragments (PTX ISA, mma.m16n8k8 .tf32), with
@@ -313,58 +316,60 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
                      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Warp tile of (16*RM) x (8*RN) outputs.  A(m,k) = Ab[arow(m) + k*ak] and
-// B(k,n) = Bb[k*bk + bcol(n)], where the row (column) offsets are the
-// stage's RowSplit offsets on the split side (split_a: rows of A, else
-// columns of B) and m*am (n*bn) otherwise; offsets are taken once per tile.
-// Loop bounds warp-uniform; lanes outside M, N or K load zeros.
+// Warp tile of (16*RM) x (8*RN) outputs over pre-split operands.
+// A(m,k) = Ab[arow(m) + k*ak] and B(k,n) = Bb[k*bk + bcol(n)], where the row
+// (column) offsets are the stage's RowSplit offsets on the split side
+// (split_a: rows of A, else columns of B) and m*am (n*bn) otherwise, taken
+// once per tile.  Loop bounds warp-uniform; lanes outside M, N or K use zeros.
 template <int RM, int RN>
-__device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const float *Ab, int am,
-                                                 int ak, const float *Bb, int bk, int bn,
+__device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const float2 *Ab, int am,
+                                                 int ak, const float2 *Bb, int bk, int bn,
                                                  const RowSplit &rs, bool split_a, int K, int M,
                                                  int N, int m0, int n0, int g, int t)
 {
-        int64_t arow[RM][2], bcol[RN];
-        bool mok[RM][2], nok[RN];
+        // 32-bit element offsets from the tile's bases (a block and its
+        // intermediates are far below 2^31 elements); -1 marks a lane outside
+        // M or N
+        int ao[RM][2], bo[RN];
 #pragma unroll
         for (int i = 0; i < RM; ++i)
 #pragma unroll
                 for (int r = 0; r < 2; ++r) {
                         const int m = m0 + 16 * i + 8 * r + g;
-                        mok[i][r] = m < M;
-                        const int mm = mok[i][r] ? m : 0;
-                        arow[i][r] = split_a ? rs.a_off(mm) : (int64_t) mm * am;
+                        ao[i][r] = m < M ? (int) (split_a ? rs.a_off(m) : (int64_t) m * am) + t * ak : -1;
                 }
 #pragma unroll
         for (int j = 0; j < RN; ++j) {
                 const int n = n0 + 8 * j + g;
-                nok[j] = n < N;
-                const int nn = nok[j] ? n : 0;
-                bcol[j] = split_a ? (int64_t) nn * bn : rs.a_off(nn);
+                bo[j] = n < N ? (int) (split_a ? (int64_t) n * bn : rs.a_off(n)) + t * bk : -1;
         }
-        for (int k0 = 0; k0 < K; k0 += 8) {
-                const int kk[2] = {k0 + t, k0 + t + 4};
+        const int a4 = 4 * ak, b4 = 4 * bk;
+        const float2 zero = make_float2(0.f, 0.f);
+        for (int k0 = 0, ka = 0, kb = 0; k0 < K; k0 += 8, ka += 2 * a4, kb += 2 * b4) {
+                const bool k0ok = k0 + t < K, k1ok = k0 + t + 4 < K;
                 uint32_t ah[RM][4], al[RM][4], bh[RN][2], bl[RN][2];
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
-                        for (int c = 0; c < 2; ++c)
-#pragma unroll
-                                for (int r = 0; r < 2; ++r) {
-                                        const float v = (mok[i][r] && kk[c] < K)
-                                                                ? Ab[arow[i][r] + (int64_t) kk[c] * ak]
-                                                                : 0.f;
-                                        split_tf32(v, ah[i][r + 2 * c], al[i][r + 2 * c]);
-                                }
-#pragma unroll
-                for (int j = 0; j < RN; ++j)
-#pragma unroll
-                        for (int c = 0; c < 2; ++c) {
-                                const float v = (nok[j] && kk[c] < K)
-                                                        ? Bb[(int64_t) kk[c] * bk + bcol[j]]
-                                                        : 0.f;
-                                split_tf32(v, bh[j][c], bl[j][c]);
+                        for (int r = 0; r < 2; ++r) {
+                                const bool ok = ao[i][r] >= 0;
+                                const float2 v0 = (ok && k0ok) ? Ab[ao[i][r] + ka] : zero;
+                                const float2 v1 = (ok && k1ok) ? Ab[ao[i][r] + ka + a4] : zero;
+                                ah[i][r] = __float_as_uint(v0.x);
+                                al[i][r] = __float_as_uint(v0.y);
+                                ah[i][r + 2] = __float_as_uint(v1.x);
+                                al[i][r + 2] = __float_as_uint(v1.y);
                         }
+#pragma unroll
+                for (int j = 0; j < RN; ++j) {
+                        const bool ok = bo[j] >= 0;
+                        const float2 v0 = (ok && k0ok) ? Bb[bo[j] + kb] : zero;
+                        const float2 v1 = (ok && k1ok) ? Bb[bo[j] + kb + b4] : zero;
+                        bh[j][0] = __float_as_uint(v0.x);
+                        bl[j][0] = __float_as_uint(v0.y);
+                        bh[j][1] = __float_as_uint(v1.x);
+                        bl[j][1] = __float_as_uint(v1.y);
+                }
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -376,14 +381,25 @@ __device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const fl
         }
 }
 
-// The grouped stage of the FP64 path for FP32 data.  The GEMM is taken in the
-// orientation that puts the larger of M and N on the tile's 16-row side.
-template <bool ACC, int RM, int RN, int NW>
-__device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int rows, int ldop,
-                                                    int G, const int64_t *opoff,
-                                                    const float *__restrict__ ops,
-                                                    const float *in, int in_gs, float *out,
-                                                    int out_gs, const float *scale, bool swap)
+__device__ __forceinline__ void store_out(float2 *p, float v, float sc, bool acc)
+{
+        *p = split_tf32(sc * v);   // intermediates: split once, here
+}
+
+__device__ __forceinline__ void store_out(float *p, float v, float sc, bool acc)
+{
+        *p = acc ? *p + v : sc * v;   // the output tile accumulates in FP32
+}
+
+// The grouped stage of the FP64 path for pre-split operands.  The GEMM is
+// taken in the orientation that puts the larger of M and N on the tile's
+// 16-row side.
+template <bool ACC, int RM, int RN, int NW, class OutT>
+__device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows, int ldop, int G,
+                                                  const int64_t *opoff,
+                                                  const float2 *__restrict__ ops,
+                                                  const float2 *in, int in_gs, OutT *out,
+                                                  int out_gs, const float *scale, bool swap)
 {
         int M, N, K, ak, bk, bn, cn;
         RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
@@ -424,10 +440,10 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) d[i][j][q] = 0.f;
                 for (int gg = g0; gg < g1; ++gg) {
-                        const float *op = ops + opoff[gg];
-                        const float *tin = in + gg * in_gs;
-                        const float *Ab = ax == 0 ? op : tin;
-                        const float *Bb = ax == 0 ? tin : op;
+                        const float2 *op = ops + opoff[gg];
+                        const float2 *tin = in + gg * in_gs;
+                        const float2 *Ab = ax == 0 ? op : tin;
+                        const float2 *Bb = ax == 0 ? tin : op;
                         if (swap)
                                 warp_tile_tf32x3<RM, RN>(d, Bb, bn, bk, Ab, ak, 1, rs, false, K, Mt, Nt,
                                                          m0, n0, g, t);
@@ -436,7 +452,7 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
                                                          m0, n0, g, t);
                 }
                 const float sc = (!ACC && scale) ? scale[g0] : 1.f;
-                float *Cb = out + (ACC ? 0 : g0 * out_gs);
+                OutT *Cb = out + (ACC ? 0 : g0 * out_gs);
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -450,19 +466,18 @@ __device__ __forceinline__ void grouped_stage_f32_t(int ax, const int *w, int ro
                                                 const int ncol = n0 + 8 * j + 2 * t + h;
                                                 if (ncol >= Nt) continue;
                                                 // C(m, n) with (m, n) = swap ? (ncol, mc) : (mc, ncol)
-                                                float *cp = swap ? Cb + rs.c_off(ncol) + (int64_t) mc * cn
-                                                                 : Cb + rs.c_off(mc) + (int64_t) ncol * cn;
-                                                const float v = d[i][j][2 * r + h];
-                                                *cp = ACC ? *cp + v : sc * v;
+                                                OutT *cp = swap ? Cb + rs.c_off(ncol) + (int64_t) mc * cn
+                                                                : Cb + rs.c_off(mc) + (int64_t) ncol * cn;
+                                                store_out(cp, d[i][j][2 * r + h], sc, ACC);
                                         }
                         }
         }
 }
 
-template <bool ACC, int NW>
+template <bool ACC, int NW, class OutT>
 __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
-                                              const int64_t *opoff, const float *__restrict__ ops,
-                                              const float *in, int in_gs, float *out, int out_gs,
+                                              const int64_t *opoff, const float2 *__restrict__ ops,
+                                              const float2 *in, int in_gs, OutT *out, int out_gs,
                                               const float *scale)
 {
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
@@ -473,31 +488,48 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
         const bool swap = pw1 < pw0;
         const int Mt = swap ? N : M, Nt = swap ? M : N;
         if (Mt <= 16)
-                grouped_stage_f32_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                   out_gs, scale, swap);
+                grouped_stage_x_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                 out_gs, scale, swap);
         else if (Nt <= 8)
-                grouped_stage_f32_t<ACC, 4, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                   out_gs, scale, swap);
+                grouped_stage_x_t<ACC, 2, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                 out_gs, scale, swap);
         else
-                grouped_stage_f32_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                   out_gs, scale, swap);
+                grouped_stage_x_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                 out_gs, scale, swap);
 }
 
+// Element types of the kernel: operand storage T, the output tile's
+// accumulator and the term prefactors.
+template <class T>
+struct Elem;
+template <>
+struct Elem<double> {
+        using Acc = double;
+        using Scale = double;
+};
+template <>
+struct Elem<float2> {
+        using Acc = float;
+        using Scale = float;
+};
+
 // Shared buffer capacities (elements) of a configuration for element type T:
-// the output tile is the plan's; FP32 fits twice the staged block and
-// intermediates in the same bytes.
+// the output tile is the plan's; the staged block and intermediates take the
+// configuration's bytes (a float2 pair is as wide as a double).
 template <class Cfg, class T>
 struct Caps {
         static constexpr int kOut = Cfg::kOut;
         static constexpr int kPsi = Cfg::kPsi * (int) (sizeof(double) / sizeof(T));
         static constexpr int kW = Cfg::kW * (int) (sizeof(double) / sizeof(T));
+        static_assert(sizeof(T) == sizeof(double), "operands are 8 bytes wide");
 };
 
 template <class Cfg, class T>
 constexpr size_t smem_bytes_t()
 {
-        return sizeof(T) * (Caps<Cfg, T>::kOut + Caps<Cfg, T>::kPsi + Caps<Cfg, T>::kW + kGMax) +
-               sizeof(int64_t) * 3 * kGMax + 64;
+        return sizeof(typename Elem<T>::Acc) * Caps<Cfg, T>::kOut +
+               sizeof(T) * (Caps<Cfg, T>::kPsi + Caps<Cfg, T>::kW) +
+               sizeof(typename Elem<T>::Scale) * kGMax + sizeof(int64_t) * 3 * kGMax + 64;
 }
 
 template <class Cfg, class T>
@@ -510,11 +542,13 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
 {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         using C = Caps<Cfg, T>;
-        T *OUT = reinterpret_cast<T *>(smem_raw);
+        using Acc = typename Elem<T>::Acc;
+        using Scale = typename Elem<T>::Scale;
+        Acc *OUT = reinterpret_cast<Acc *>(smem_raw);
         constexpr int kThreads = Cfg::kThreads, NW = Cfg::kThreads / 32;
-        T *PSI = OUT + C::kOut;
+        T *PSI = reinterpret_cast<T *>(OUT + C::kOut);
         T *W = PSI + C::kPsi;
-        T *PREF = W + C::kW;
+        Scale *PREF = reinterpret_cast<Scale *>(W + C::kW);
         int64_t *OPOFF = reinterpret_cast<int64_t *>(PREF + kGMax);   // [3][kGMax]
         int *UNIT = reinterpret_cast<int *>(OPOFF + 3 * kGMax);
         const int tid = threadIdx.x;
@@ -533,7 +567,7 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                 const int ext[3] = {un.at, un.bt, un.ct};
                 const int row0[3] = {un.a0, un.b0, un.c0};
                 const int st = ext[0] * ext[1] * ext[2];
-                for (int e = tid; e < st; e += kThreads) OUT[e] = T(0);
+                for (int e = tid; e < st; e += kThreads) OUT[e] = Acc(0);
                 __syncthreads();
                 for (int p = un.p0; p < un.p1; ++p) {
                         const HeffPair pr = pairs[p];
@@ -568,7 +602,7 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                                         const HeffTask &tk = tasks[pr.t0 + t0 + tid];
                                         for (int s = 0; s < 3; ++s)
                                                 OPOFF[s * kGMax + tid] = tk.op_off[ax[s]] + row0[ax[s]];
-                                        PREF[tid] = (T) tk.pref;
+                                        PREF[tid] = (Scale) tk.pref;
                                 }
                                 __syncthreads();
                                 if (nst == 3) {
@@ -1068,18 +1102,24 @@ static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const T *x, c
         return T3NS_OK;
 }
 
-__global__ void to_f32_kernel(const double *__restrict__ a, float *__restrict__ b, int64_t n)
+// b[i] = {hi, lo}: hi = tf32(a[i]), lo = tf32(a[i] - hi), the remainder
+// taken in FP64 so lo carries the bits FP32 would round away.
+__global__ void split_tf32_kernel(const double *__restrict__ a, float2 *__restrict__ b, int64_t n)
 {
         for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
-             i += (int64_t) gridDim.x * blockDim.x)
-                b[i] = (float) a[i];
+             i += (int64_t) gridDim.x * blockDim.x) {
+                const double v = a[i];
+                const float hi = __uint_as_float(to_tf32((float) v));
+                const float lo = __uint_as_float(to_tf32((float) (v - (double) hi)));
+                b[i] = make_float2(hi, lo);
+        }
 }
 
-int convert_to_f32(const double *a, float *b, int64_t n, cudaStream_t s)
+int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s)
 {
         if (n <= 0) return T3NS_OK;
         const int grid = (int) std::min<int64_t>((n + 255) / 256, 148 * 16);
-        to_f32_kernel<<<grid, 256, 0, s>>>(a, b, n);
+        split_tf32_kernel<<<grid, 256, 0, s>>>(a, b, n);
         T3NS_CUDA_TRY(cudaGetLastError());
         return T3NS_OK;
 }
@@ -1090,20 +1130,20 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         const DeviceTiles &dt = dp.tiles[dp.active];
         if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
         const bool split = precision == T3NS_PREC_3XTF32;
-        if (split && (!dp.ops32 || !dp.x32))
+        if (split && (!dp.ops_split || !dp.x_split))
                 return set_error(T3NS_E_ARG, "matvec: split precision is not set up on this plan");
         if (precision != T3NS_PREC_FP64 && !split)
                 return set_error(T3NS_E_ARG, "matvec: unsupported precision");
         T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
         if (launches) *launches = 0;
         if (dt.n_units == 0) return T3NS_OK;
-        if (split) T3NS_TRY(convert_to_f32(x, dp.x32, dp.size, s));
+        if (split) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
         static_assert(kNumCfgs == 2, "one launch branch per configuration");
         int rc;
         if (split)
-                rc = dp.active == 0 ? launch_cfg<CfgLarge, float>(dp, dt, dp.x32, dp.ops32, y, s)
-                                    : launch_cfg<CfgSmall, float>(dp, dt, dp.x32, dp.ops32, y, s);
+                rc = dp.active == 0 ? launch_cfg<CfgLarge, float2>(dp, dt, dp.x_split, dp.ops_split, y, s)
+                                    : launch_cfg<CfgSmall, float2>(dp, dt, dp.x_split, dp.ops_split, y, s);
         else
                 rc = dp.active == 0 ? launch_cfg<CfgLarge, double>(dp, dt, x, dp.ops, y, s)
                                     : launch_cfg<CfgSmall, double>(dp, dt, x, dp.ops, y, s);

@@ -102,8 +102,8 @@ struct DevicePlan {
         int nblocks = 0;
         int64_t size = 0;
         double *ops = nullptr;
-        float *ops32 = nullptr;                   // FP32 copy for the split-precision matvec
-        float *x32 = nullptr;                     // FP32 input staging
+        float2 *ops_split = nullptr;              // {hi, lo} TF32 split of the operators
+        float2 *x_split = nullptr;                // {hi, lo} split of the matvec input
         int64_t *blk_off = nullptr;
         int4 *edims = nullptr;
         int *task_ptr = nullptr;
@@ -128,7 +128,7 @@ int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStrea
 // The matvec in precision T3NS_PREC_FP64 or T3NS_PREC_3XTF32 (FP64 in and out).
 int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
                 int *launches);
-int convert_to_f32(const double *a, float *b, int64_t n, cudaStream_t s);
+int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s);
 int launch_heff_diag(const DevicePlan &dp, double *diag, cudaStream_t s);
 
 }  // namespace t3ns

@@ -57,8 +57,8 @@ struct Request {
 
 }  // namespace
 
-// Device bytes a solve of `desc` needs: operators (and their FP32 copy in
-// split precision), the plan's term table (upper bound: every instruction of
+// Device bytes a solve of `desc` needs: operators (and their {hi, lo} copy
+// in split precision), the plan's term table (upper bound: every instruction of
 // every combination present) and tilings, the plan's staging vectors, and
 // the Davidson basis V, VA plus its work vectors.
 int64_t estimate_solve_bytes(const t3ns_heff_desc *d, int precision, int max_vecs)
@@ -74,10 +74,10 @@ int64_t estimate_solve_bytes(const t3ns_heff_desc *d, int precision, int max_vec
         for (int64_t c = 0; c < d->combo_ptr[npairs]; ++c)
                 tasks += d->MPOc_beg[d->combo_mpo[c] + 1] - d->MPOc_beg[d->combo_mpo[c]];
         const bool split = precision == T3NS_PREC_3XTF32;
-        int64_t b = op_elems * (split ? 12 : 8);
+        int64_t b = op_elems * (split ? 16 : 8);               // FP64 (+ {hi, lo} pairs)
         b += tasks * (int64_t) sizeof(HeffTask);
         b += kNumCfgs * npairs * (int64_t) (sizeof(HeffPair) + 4 * sizeof(HeffUnit));
-        b += n * (16 + (split ? 4 : 0));                      // plan staging (+ FP32 input)
+        b += n * (16 + (split ? 8 : 0));                      // plan staging (+ split input)
         b += n * 8 * (2 * (int64_t) std::max(max_vecs, 3) + 6); // basis + work vectors
         return b + b / 20 + (16 << 20);                      // 5% + 16 MiB slack
 }
