@@ -52,10 +52,10 @@ constexpr double kPairVisitCost = 4e4;   // FLOP-equivalent of one (unit, pair) 
 // Kernel configurations.  The large one (one 512-thread CTA per SM, 208 KB of
 // shared buffers) tiles fewer blocks and hides latency with 16 warps; the
 // small one (two 256-thread CTAs per SM) suits steps of many small blocks.
-// Both use all 64K registers of an SM (124 per thread at most).
+// Both fit the 64K registers of an SM (at most 128 per thread).
 struct CfgLarge {
         static constexpr int kThreads = 512, kMinBlocks = 1;
-        static constexpr int kOut = 8192, kPsi = 4096, kW = 14336;
+        static constexpr int kOut = 8192, kPsi = 2048, kW = 16384;
 };
 struct CfgSmall {
         static constexpr int kThreads = 256, kMinBlocks = 2;
