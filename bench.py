@@ -11,7 +11,9 @@ same step (`split_precision`), whole sweeps of the reference driver linked
 against the drop-in with FP64 and with split-precision matvecs plus FP64
 defect correction (`sweep`: sweep seconds and final-energy difference), and
 the engine's request loop under a Poisson stream of solves (`serving`:
-p50/p99 latency, solves/s).
+p50/p99 latency, solves/s), and the renormalised-operator updates and the
+decomposition's SVDs through their host calls on the captured sweep calls
+(`updates_and_decomposition`).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -344,6 +346,87 @@ def davidson_comparison(path=None, max_its=100, seed=7):
     return out
 
 
+def other_rows_measurement(reps=3):
+    """The renormalised-operator updates and the decomposition's
+    factorisations through their host C-ABI calls (host arrays in and out,
+    uploads, device allocations and the kernel: what the drop-in pays per
+    call), on every captured call of the Hubbard and 12-orbital QC sweeps:
+    algorithmic GFLOP and GPU seconds (best of `reps` per call); the SVDs
+    also timed through the reference's LAPACK (OpenBLAS LAPACKE_dgesdd) on the
+    host for comparison.  None if the captures are absent."""
+    import ctypes as C
+    from t3ns_b200 import native, updates
+    from t3ns_b200.stepfile import read_step
+    caps = os.path.join(ROOT, "oracle", "_ref", "captures")
+    out = {}
+
+    def best(fn):
+        t = []
+        for _ in range(reps + 1):
+            t0 = time.perf_counter()
+            fn()
+            t.append(time.perf_counter() - t0)
+        return min(t[1:])
+
+    for kind in ("pupdate", "bupdate"):
+        files = sorted(glob.glob(os.path.join(caps, "pupdate_*", f"{kind}_*.t3c")))
+        files = [f for f in files if os.path.exists(f.replace(".t3c", ".sched"))]
+        if not files:
+            return None
+        flops = secs = 0.0
+        for f in files:
+            rec, sch = read_step(f), read_step(f.replace(".t3c", ".sched"))
+            if kind == "pupdate":
+                flops += updates.pupdate_flops(sch)
+                secs += best(lambda: updates.pupdate_host(sch, rec["T.tel"], rec["ops0.tel"]))
+            else:
+                flops += updates.bupdate_flops(sch)
+                secs += best(lambda: updates.bupdate_host(sch, rec["T.tel"], rec["ops0.tel"],
+                                                          rec["ops1.tel"]))
+        out[kind] = {"calls": len(files), "gflop": flops / 1e9, "gpu_seconds_e2e": secs,
+                     "gflop_per_s_e2e": flops / secs / 1e9}
+
+    lib = native.load()
+    lib.t3ns_gesdd_host.argtypes = [C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                    C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    libdir = os.path.join(os.path.dirname(np.__file__), "..", "opencv_python_headless.libs")
+    blas = glob.glob(os.path.join(libdir, "libopenblas*.so"))
+    for pat in ("libquadmath*.so*", "libgfortran*.so*"):   # OpenBLAS's Fortran runtime
+        for dep in glob.glob(os.path.join(libdir, pat)):
+            C.CDLL(dep, mode=C.RTLD_GLOBAL)
+    cpu = C.CDLL(blas[0]) if blas else None
+    if cpu is not None:
+        cpu.LAPACKE_dgesdd.argtypes = [C.c_int, C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                       C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    files = sorted(glob.glob(os.path.join(caps, "dense_*", "gesdd_*.t3c")))
+    gpu_s = cpu_s = 0.0
+    largest = (0, 0)
+    for f in files:
+        r = read_step(f)
+        m, n = int(r["gesdd.m"][0]), int(r["gesdd.n"][0])
+        jobz = chr(int(r["gesdd.jobz"][0]))
+        k = min(m, n)
+        if k == 0:
+            continue
+        largest = max(largest, (m, n), key=lambda x: x[0] * x[1])
+        s_ = np.zeros(k)
+        u = np.zeros(max(m * k, 1))
+        vt = np.zeros(max(k * n, 1))
+
+        def run(fn):
+            def go():
+                a = np.array(r["gesdd.a"])
+                fn(jobz.encode(), m, n, a.ctypes.data, m, s_.ctypes.data, u.ctypes.data, m,
+                   vt.ctypes.data, k)
+            return go
+        gpu_s += best(run(lambda *x: native.check(lib.t3ns_gesdd_host(*x), "gesdd")))
+        if cpu is not None:
+            cpu_s += best(run(lambda *x: cpu.LAPACKE_dgesdd(102, *x)))
+    out["gesdd"] = {"calls": len(files), "largest": list(largest), "gpu_seconds_e2e": gpu_s,
+                    "reference_lapack_seconds": cpu_s if cpu is not None else None}
+    return out
+
+
 def serving_stream():
     """The engine's request loop under a Poisson stream of 128 independent
     ground-state solves (mean 4 arrivals/s; solves drawn from the captured
@@ -470,6 +553,8 @@ def main():
             out["sweep"] = sweep_comparison()
         if not args.no_serving:
             out["serving"] = serving_stream()
+        if not args.no_sweep:
+            out["updates_and_decomposition"] = other_rows_measurement()
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

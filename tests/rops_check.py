@@ -5,19 +5,9 @@ it through the C ABI, sum unique operators as the reference does, apply the
 reference's zero-block removal (kick_zero_blocks, src/sparseblocks.c:73-107)
 and compare with the reference's output captured in the same file ("ops1.*"
 records for the physical update, "ops2.*" for the branching one)."""
-import ctypes as C
-
 import numpy as np
 
-from t3ns_b200 import native
-
-
-class PupdateDesc(C.Structure):
-    _fields_ = [("is_left", C.c_int), ("nunits", C.c_int), ("unit_ptr", C.c_void_p),
-                ("nentries", C.c_int), ("dims", C.c_void_p), ("t_off", C.c_void_p),
-                ("ta_off", C.c_void_p), ("pref", C.c_void_p), ("op_ptr", C.c_void_p),
-                ("old_off", C.c_void_p), ("new_off", C.c_void_p), ("t_elems", C.c_int64),
-                ("old_elems", C.c_int64), ("new_elems", C.c_int64)]
+from t3ns_b200 import updates
 
 
 def ops_structure(rec, i):
@@ -60,24 +50,7 @@ def emulate_pupdate(rec, sch):
 
 
 def run_pupdate_gpu(rec, sch):
-    lib = native.load()
-    lib.t3ns_pupdate_host.argtypes = [C.POINTER(PupdateDesc), C.c_void_p, C.c_void_p, C.c_void_p]
-    keep = {k: np.ascontiguousarray(sch[k]) for k in sch}
-    d = PupdateDesc()
-    d.is_left = int(sch["pu.is_left"][0])
-    d.nunits = len(keep["pu.unit_ptr"]) - 1
-    d.unit_ptr = keep["pu.unit_ptr"].ctypes.data
-    d.nentries = len(keep["pu.pref"])
-    for f in ("dims", "t_off", "ta_off", "pref", "op_ptr", "old_off", "new_off"):
-        setattr(d, f, keep["pu." + f].ctypes.data)
-    T = np.ascontiguousarray(rec["T.tel"])
-    old = np.ascontiguousarray(rec["ops0.tel"])
-    d.t_elems, d.old_elems = T.size, old.size
-    d.new_elems = int(keep["pu.new_base"][-1])
-    new = np.empty(max(d.new_elems, 1))
-    native.check(lib.t3ns_pupdate_host(C.byref(d), T.ctypes.data, old.ctypes.data,
-                                       new.ctypes.data), "pupdate_host")
-    return new[:d.new_elems]
+    return updates.pupdate_host(sch, rec["T.tel"], rec["ops0.tel"])
 
 
 def kick_compare(rec, idx, pre):
@@ -125,15 +98,6 @@ def kick_and_compare(rec, sch, new):
     return kick_compare(rec, 1, out)
 
 
-class BupdateDesc(C.Structure):
-    _fields_ = [("ax", C.c_int * 3), ("nunits", C.c_int), ("unit_ptr", C.c_void_p),
-                ("nentries", C.c_int), ("dims", C.c_void_p), ("t_off", C.c_void_p),
-                ("ta_off", C.c_void_p), ("pref", C.c_void_p), ("op_ptr", C.c_void_p),
-                ("o1_off", C.c_void_p), ("o2_off", C.c_void_p), ("new_off", C.c_void_p),
-                ("t_elems", C.c_int64), ("o1_elems", C.c_int64), ("o2_elems", C.c_int64),
-                ("new_elems", C.c_int64)]
-
-
 def _block3(arr, off, d):
     """Column-major block of dims d as an array indexed [i0, i1, i2]."""
     n = d[0] * d[1] * d[2]
@@ -167,27 +131,7 @@ def emulate_bupdate(rec, sch):
 
 
 def run_bupdate_gpu(rec, sch):
-    lib = native.load()
-    lib.t3ns_bupdate_host.argtypes = [C.POINTER(BupdateDesc), C.c_void_p, C.c_void_p,
-                                      C.c_void_p, C.c_void_p]
-    keep = {k: np.ascontiguousarray(sch[k]) for k in sch}
-    d = BupdateDesc()
-    for i in range(3):
-        d.ax[i] = int(keep["bu.ax"][i])
-    d.nunits = len(keep["bu.unit_ptr"]) - 1
-    d.unit_ptr = keep["bu.unit_ptr"].ctypes.data
-    d.nentries = len(keep["bu.pref"])
-    for f in ("dims", "t_off", "ta_off", "pref", "op_ptr", "o1_off", "o2_off", "new_off"):
-        setattr(d, f, keep["bu." + f].ctypes.data)
-    T = np.ascontiguousarray(rec["T.tel"])
-    o1 = np.ascontiguousarray(rec["ops0.tel"])
-    o2 = np.ascontiguousarray(rec["ops1.tel"])
-    d.t_elems, d.o1_elems, d.o2_elems = T.size, o1.size, o2.size
-    d.new_elems = int(keep["bu.unique_base"][-1])
-    new = np.empty(max(d.new_elems, 1))
-    native.check(lib.t3ns_bupdate_host(C.byref(d), T.ctypes.data, o1.ctypes.data,
-                                       o2.ctypes.data, new.ctypes.data), "bupdate_host")
-    return new[:d.new_elems]
+    return updates.bupdate_host(sch, rec["T.tel"], rec["ops0.tel"], rec["ops1.tel"])
 
 
 def sum_unique(rec, sch, unique):
