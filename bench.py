@@ -260,7 +260,8 @@ def run_engine(args, rank, world):
                             "speedup_vs_fp64": t_total / t_split,
                             "rel_err_vs_fp64": split_err, "kernel_config": split_cfg,
                             "autotune_ms": split_tune,
-                            "arithmetic": "3xTF32 products of FP32 data, FP32 accumulation"},
+                            "arithmetic": "3xTF32 products of pre-split {hi, lo} TF32 pairs, "
+                                          "FP32 accumulation"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
