@@ -59,13 +59,13 @@ struct CfgLarge {
 };
 struct CfgSmall {
         static constexpr int kThreads = 256, kMinBlocks = 2;
-        static constexpr int kOut = 2048, kPsi = 3072, kW = 8192;
+        static constexpr int kOut = 3072, kPsi = 1024, kW = 9472;
 };
 const KernelCfg kCfgs[kNumCfgs] = {
         {CfgLarge::kThreads, CfgLarge::kMinBlocks, CfgLarge::kOut, CfgLarge::kPsi, CfgLarge::kW,
          "fp64-512x1-out8192"},
         {CfgSmall::kThreads, CfgSmall::kMinBlocks, CfgSmall::kOut, CfgSmall::kPsi, CfgSmall::kW,
-         "fp64-256x2-out2048"},
+         "fp64-256x2-out3072"},
 };
 
 
