@@ -55,7 +55,7 @@ constexpr double kPairVisitCost = 4e4;   // FLOP-equivalent of one (unit, pair) 
 // Both fit the 64K registers of an SM (at most 128 per thread).
 struct CfgLarge {
         static constexpr int kThreads = 512, kMinBlocks = 1;
-        static constexpr int kOut = 8192, kPsi = 2048, kW = 16384;
+        static constexpr int kOut = 8192, kPsi = 1024, kW = 17408;
 };
 struct CfgSmall {
         static constexpr int kThreads = 256, kMinBlocks = 2;
