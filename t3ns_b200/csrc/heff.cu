@@ -201,7 +201,8 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
                                                 const int64_t *opoff,
                                                 const double *__restrict__ ops, const double *in,
                                                 int in_gs, double *out, int out_gs,
-                                                const double *scale)
+                                                const double *scale, double *scratch,
+                                                int scratch_cap)
 {
         int M, N, K, ak, bk, bn, cn;
         RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
@@ -220,23 +221,36 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
         }
         const int mt = (M + 8 * RM - 1) / (8 * RM), nt = (N + 8 * RN - 1) / (8 * RN);
         const int tiles = mt * nt;
-        const int items = (ACC ? 1 : G) * tiles;
+        // The accumulating stage sums the G terms inside each warp.  When its
+        // output has fewer tiles than the CTA has warps, the terms are dealt
+        // out to P parts (term g to part g % P) so P warps share a tile; the
+        // parts' partial tiles go to scratch and are added in part order
+        // (deterministic).
+        int P = 1;
+        const int MN = M * N;
+        if (ACC && tiles < NW && G > 1 && scratch) {
+                P = min(G, NW / tiles);
+                P = min(P, scratch_cap / max(MN, 1));
+                if (P < 2) P = 1;
+        }
+        const int items = (ACC ? P : G) * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int lr = lane >> 2, lc = lane & 3;
         const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt;
         for (int it = warp; it < items; it += NW) {
                 int tile, tm;
-                const int g0 = ACC ? 0 : fast_divmod(it, tiles, r_tiles, tile);
-                if (ACC) tile = it;
+                const int q = fast_divmod(it, tiles, r_tiles, tile);   // term (or part)
+                const int g0 = q;
                 const int tn = fast_divmod(tile, mt, r_mt, tm);
                 const int g1 = ACC ? G : g0 + 1;
+                const int gstep = ACC ? P : 1;
                 const int m0 = tm * 8 * RM, n0 = tn * 8 * RN;
                 double d[RM][RN][2];
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
                         for (int j = 0; j < RN; ++j) d[i][j][0] = d[i][j][1] = 0.0;
-                for (int g = g0; g < g1; ++g) {
+                for (int g = g0; g < g1; g += gstep) {
                         const double *op = ops + opoff[g];
                         const double *tin = in + g * in_gs;
                         const double *Ab = ax == 0 ? op : tin;
@@ -256,10 +270,25 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
 #pragma unroll
                                 for (int h = 0; h < 2; ++h) {
                                         if (nc0 + h >= N) continue;
+                                        if (ACC && P > 1) {
+                                                scratch[(int64_t) q * MN + mc + (nc0 + h) * M] = d[i][j][h];
+                                                continue;
+                                        }
                                         double *cp = crow + (nc0 + h) * cn;
                                         *cp = ACC ? *cp + d[i][j][h] : sc * d[i][j][h];
                                 }
                         }
+                }
+        }
+        if (ACC && P > 1) {
+                __syncthreads();
+                const float r_m = 1.0f / M;
+                for (int e = threadIdx.x; e < MN; e += NW * 32) {
+                        int m;
+                        const int n = fast_divmod(e, M, r_m, m);
+                        double sum = 0.0;
+                        for (int p = 0; p < P; ++p) sum += scratch[(int64_t) p * MN + e];
+                        out[rs.c_off(m) + (int64_t) n * cn] += sum;
                 }
         }
 }
@@ -271,16 +300,20 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                                               const int64_t *opoff,
                                               const double *__restrict__ ops, const double *in,
                                               int in_gs, double *out, int out_gs,
-                                              const double *scale)
+                                              const double *scale, double *scratch = nullptr,
+                                              int scratch_cap = 0)
 {
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
         if (M <= 8)
-                grouped_stage_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+                grouped_stage_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
+                                               scratch, scratch_cap);
         else if (N <= 8)
-                grouped_stage_t<ACC, 4, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+                grouped_stage_t<ACC, 4, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
+                                               scratch, scratch_cap);
         else
-                grouped_stage_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale);
+                grouped_stage_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
+                                               scratch, scratch_cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -478,7 +511,7 @@ template <bool ACC, int NW, class OutT>
 __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
                                               const int64_t *opoff, const float2 *__restrict__ ops,
                                               const float2 *in, int in_gs, OutT *out, int out_gs,
-                                              const float *scale)
+                                              const float *scale, float2 * = nullptr, int = 0)
 {
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
@@ -612,16 +645,17 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                                         grouped_stage<false, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
                                                              OPOFF + kGMax, ops, W1, s1, W2, s2, PREF);
                                         __syncthreads();
+                                        // stage 3 reads W2 only: W1's share is its scratch
                                         grouped_stage<true, NW>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
                                                             OPOFF + 2 * kGMax, ops, W2, s2, OUT, 0,
-                                                            nullptr);
+                                                            nullptr, W1, G * s1);
                                 } else {
                                         grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
                                                              ops, in0, 0, W1, s1, PREF);
                                         __syncthreads();
                                         grouped_stage<true, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
                                                             OPOFF + kGMax, ops, W1, s1, OUT, 0,
-                                                            nullptr);
+                                                            nullptr, W1 + G * s1, C::kW - G * s1);
                                 }
                                 __syncthreads();
                         }
