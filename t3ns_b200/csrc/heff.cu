@@ -432,7 +432,8 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
                                                   const int64_t *opoff,
                                                   const float2 *__restrict__ ops,
                                                   const float2 *in, int in_gs, OutT *out,
-                                                  int out_gs, const float *scale, bool swap)
+                                                  int out_gs, const float *scale, bool swap,
+                                                  float *scratch, int scratch_cap)
 {
         int M, N, K, ak, bk, bn, cn;
         RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
@@ -454,16 +455,25 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
         const int Mt = swap ? N : M, Nt = swap ? M : N;
         const int mt = (Mt + 16 * RM - 1) / (16 * RM), nt = (Nt + 8 * RN - 1) / (8 * RN);
         const int tiles = mt * nt;
-        const int items = (ACC ? 1 : G) * tiles;
+        // terms of the accumulating stage dealt to P parts when its output
+        // has fewer tiles than warps (as in the FP64 stage)
+        int P = 1;
+        const int MN = M * N;
+        if (ACC && tiles < NW && G > 1 && scratch) {
+                P = min(G, NW / tiles);
+                P = min(P, scratch_cap / max(MN, 1));
+                if (P < 2) P = 1;
+        }
+        const int items = (ACC ? P : G) * tiles;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int g = lane >> 2, t = lane & 3;
         const float r_tiles = 1.0f / tiles, r_mt = 1.0f / mt;
         for (int it = warp; it < items; it += NW) {
                 int tile, tm;
-                const int g0 = ACC ? 0 : fast_divmod(it, tiles, r_tiles, tile);
-                if (ACC) tile = it;
+                const int g0 = fast_divmod(it, tiles, r_tiles, tile);   // term (or part)
                 const int tn = fast_divmod(tile, mt, r_mt, tm);
                 const int g1 = ACC ? G : g0 + 1;
+                const int gstep = ACC ? P : 1;
                 const int m0 = tm * 16 * RM, n0 = tn * 8 * RN;
                 float d[RM][RN][4];
 #pragma unroll
@@ -472,7 +482,7 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
                         for (int j = 0; j < RN; ++j)
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) d[i][j][q] = 0.f;
-                for (int gg = g0; gg < g1; ++gg) {
+                for (int gg = g0; gg < g1; gg += gstep) {
                         const float2 *op = ops + opoff[gg];
                         const float2 *tin = in + gg * in_gs;
                         const float2 *Ab = ax == 0 ? op : tin;
@@ -498,6 +508,12 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
                                         for (int h = 0; h < 2; ++h) {
                                                 const int ncol = n0 + 8 * j + 2 * t + h;
                                                 if (ncol >= Nt) continue;
+                                                if (ACC && P > 1) {
+                                                        // C(m, n) of this part in scratch
+                                                        const int m = swap ? ncol : mc, n = swap ? mc : ncol;
+                                                        scratch[(int64_t) g0 * MN + m + n * M] = d[i][j][2 * r + h];
+                                                        continue;
+                                                }
                                                 // C(m, n) with (m, n) = swap ? (ncol, mc) : (mc, ncol)
                                                 OutT *cp = swap ? Cb + rs.c_off(ncol) + (int64_t) mc * cn
                                                                 : Cb + rs.c_off(mc) + (int64_t) ncol * cn;
@@ -505,14 +521,29 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
                                         }
                         }
         }
+        if (ACC && P > 1) {
+                __syncthreads();
+                const float r_m = 1.0f / M;
+                for (int e = threadIdx.x; e < MN; e += NW * 32) {
+                        int m;
+                        const int n = fast_divmod(e, M, r_m, m);
+                        float sum = 0.f;
+                        for (int p = 0; p < P; ++p) sum += scratch[(int64_t) p * MN + e];
+                        store_out(out + rs.c_off(m) + (int64_t) n * cn, sum, 1.f, true);
+                }
+        }
 }
 
 template <bool ACC, int NW, class OutT>
 __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
                                               const int64_t *opoff, const float2 *__restrict__ ops,
                                               const float2 *in, int in_gs, OutT *out, int out_gs,
-                                              const float *scale, float2 * = nullptr, int = 0)
+                                              const float *scale, float2 *scratch = nullptr,
+                                              int scratch_cap = 0)
 {
+        // the scratch holds FP32 partial tiles: two per float2 slot
+        float *fs = reinterpret_cast<float *>(scratch);
+        const int fcap = 2 * scratch_cap;
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
         // padded work of the two orientations (16 x 8 granules)
@@ -522,13 +553,13 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
         const int Mt = swap ? N : M, Nt = swap ? M : N;
         if (Mt <= 16)
                 grouped_stage_x_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                 out_gs, scale, swap);
+                                                 out_gs, scale, swap, fs, fcap);
         else if (Nt <= 8)
                 grouped_stage_x_t<ACC, 2, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                 out_gs, scale, swap);
+                                                 out_gs, scale, swap, fs, fcap);
         else
                 grouped_stage_x_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                 out_gs, scale, swap);
+                                                 out_gs, scale, swap, fs, fcap);
 }
 
 // Element types of the kernel: operand storage T, the output tile's
