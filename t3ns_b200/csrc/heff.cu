@@ -189,6 +189,84 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
         }
 }
 
+// The accumulating stage's loop over terms g0, g0 + gstep, ... < g1 of one
+// warp tile, as warp_tile_mma per term but pipelined across terms: the K
+// loop runs ceil(K/4) steps (the last predicated when K % 4 != 0) and the
+// final step of a term already loads the first step of the next term, so a
+// term's start does not wait on its operand loads.
+template <int RM, int RN>
+__device__ __forceinline__ void warp_tile_mma_terms(double (&d)[RM][RN][2], int ax,
+                                                    const double *__restrict__ ops,
+                                                    const int64_t *opoff, const double *in,
+                                                    int in_gs, int g0, int g1, int gstep, int ak,
+                                                    const RowSplit &rs, int bk, int bn, int K,
+                                                    int M, int N, int m0, int n0, int lr, int lc)
+{
+        const int S = (K + 3) >> 2, rem = K & 3;
+        if (g0 >= g1 || S == 0) return;
+        bool mok[RM], nok[RN];
+        int64_t ao[RM], bo[RN];
+#pragma unroll
+        for (int i = 0; i < RM; ++i) {
+                const int m = m0 + 8 * i + lr;
+                mok[i] = m < M;
+                ao[i] = rs.a_off(mok[i] ? m : 0) + (int64_t) lc * ak;
+        }
+#pragma unroll
+        for (int j = 0; j < RN; ++j) {
+                const int n = n0 + 8 * j + lr;
+                nok[j] = n < N;
+                bo[j] = (int64_t) (nok[j] ? n : 0) * bn + (int64_t) lc * bk;
+        }
+        const int64_t astep = 4 * (int64_t) ak, bstep = 4 * (int64_t) bk;
+        const double *ap[RM], *bp[RN];
+        auto set_term = [&](int g) {
+                const double *op = ops + opoff[g];
+                const double *tin = in + (int64_t) g * in_gs;
+                const double *Ab = ax == 0 ? op : tin, *Bb = ax == 0 ? tin : op;
+#pragma unroll
+                for (int i = 0; i < RM; ++i) ap[i] = Ab + ao[i];
+#pragma unroll
+                for (int j = 0; j < RN; ++j) bp[j] = Bb + bo[j];
+        };
+        double a[RM], b[RN];
+        auto load = [&](int st) {
+                const bool kok = st + 1 < S || rem == 0 || lc < rem;
+#pragma unroll
+                for (int i = 0; i < RM; ++i) {
+                        a[i] = (mok[i] && kok) ? *ap[i] : 0.0;
+                        ap[i] += astep;
+                }
+#pragma unroll
+                for (int j = 0; j < RN; ++j) {
+                        b[j] = (nok[j] && kok) ? *bp[j] : 0.0;
+                        bp[j] += bstep;
+                }
+        };
+        set_term(g0);
+        load(0);
+        for (int g = g0; g < g1; g += gstep) {
+                for (int st = 0; st < S; ++st) {
+                        double ca[RM], cb[RN];
+#pragma unroll
+                        for (int i = 0; i < RM; ++i) ca[i] = a[i];
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) cb[j] = b[j];
+                        if (st + 1 < S) {
+                                load(st + 1);
+                        } else if (g + gstep < g1) {
+                                set_term(g + gstep);
+                                load(0);
+                        }
+#pragma unroll
+                        for (int i = 0; i < RM; ++i)
+#pragma unroll
+                                for (int j = 0; j < RN; ++j)
+                                        dmma_8x8x4(d[i][j][0], d[i][j][1], ca[i], cb[j]);
+                }
+        }
+}
+
 // One contraction stage for G terms.  Term g applies rows [row0, row0+rows)
 // of the operator block at ops + opoff[g] (leading dimension ldop) on axis ax
 // of `in + g * in_gs` (dims w), writing `out + g * out_gs` (scaled by
@@ -250,9 +328,12 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
                         for (int j = 0; j < RN; ++j) d[i][j][0] = d[i][j][1] = 0.0;
-                for (int g = g0; g < g1; g += gstep) {
-                        const double *op = ops + opoff[g];
-                        const double *tin = in + g * in_gs;
+                if (ACC) {
+                        warp_tile_mma_terms<RM, RN>(d, ax, ops, opoff, in, in_gs, g0, g1, gstep, ak,
+                                                    rs, bk, bn, K, M, N, m0, n0, lr, lc);
+                } else {
+                        const double *op = ops + opoff[g0];
+                        const double *tin = in + g0 * in_gs;
                         const double *Ab = ax == 0 ? op : tin;
                         const double *Bb = ax == 0 ? tin : op;
                         warp_tile_mma<RM, RN>(d, Ab, ak, rs, Bb, bk, bn, K, M, N, m0, n0, lr, lc);
