@@ -1215,11 +1215,20 @@ int tile_plan(HostPlan &hp, int cfg)
         tp.pair_ptr[hp.nblocks] = (int) tp.pairs.size();
         tp.flops_exec = flops_exec;
 
-        // heaviest units first
+        // Blocks in order of their total work, heaviest first, and the tiles
+        // of one block next to each other (heaviest first): CTAs that start
+        // together then read the same operator rows while they sit in L2.
         std::vector<int> idx(tp.units.size());
         std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(),
-                         [&](int a, int b) { return unit_work[a] > unit_work[b]; });
+        std::vector<double> block_work(hp.nblocks, 0.0);
+        for (size_t u = 0; u < tp.units.size(); ++u) block_work[tp.units[u].nb] += unit_work[u];
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+                const int na = tp.units[a].nb, nb = tp.units[b].nb;
+                if (na != nb)
+                        return block_work[na] != block_work[nb] ? block_work[na] > block_work[nb]
+                                                                : na < nb;
+                return unit_work[a] > unit_work[b];
+        });
         std::vector<HeffUnit> sorted(tp.units.size());
         for (size_t i = 0; i < idx.size(); ++i) sorted[i] = tp.units[idx[i]];
         tp.units.swap(sorted);
