@@ -3,7 +3,10 @@
 // LAPACK for (LAPACKE_dgesdd at src/siteTensor_decompose.c:1060 and :565,
 // LAPACKE_dgeqrf at :285, LAPACKE_dorgqr at :295), one symmetry sector per
 // call.  Each call runs as one CTA on the caller thread's own stream, so the
-// reference's OpenMP loop over sectors keeps several sectors in flight.
+// reference's OpenMP loop over sectors keeps several sectors in flight, and
+// costs one upload, one launch, one download and one synchronisation: the
+// thread's device workspace and pinned staging buffer are kept between
+// calls and only grow.
 //
 // SVD: one-sided (Hestenes) Jacobi on the columns of the tall orientation W
 // of A (A or A^T), parallel round-robin ordering, rotations accumulated into
@@ -138,7 +141,7 @@ svd_jacobi_kernel(int m, int n, const double *__restrict__ A, double *W, double 
                 __syncthreads();
                 if (!any) break;
         }
-        if (sweep == kMaxSweeps && tid == 0) *status = 1;
+        if (tid == 0) *status = sweep == kMaxSweeps ? 1 : 0;
 
         // norms, ranks (descending, ties by index), sorted outputs
         for (int j = warp; j < nn; j += kDenseWarps) {
@@ -312,30 +315,87 @@ org2r_kernel(int m, int n, int k, double *A, const double *__restrict__ tau)
         }
 }
 
-// Per host thread: the stream its calls run on.
-cudaStream_t thread_stream()
+// Per host thread: the stream its calls run on, a device workspace and a
+// pinned host staging buffer, both kept between calls and grown (to at least
+// twice their size) when a call needs more.  Freed when the thread exits.
+struct ThreadWork {
+        int device = -1;
+        cudaStream_t st = nullptr;
+        char *dev = nullptr, *host = nullptr;
+        size_t dev_bytes = 0, host_bytes = 0;
+        bool smem_set = false;   // large dynamic shared memory enabled for the SVD
+
+        void release()
+        {
+                if (st) cudaStreamSynchronize(st);
+                if (dev) cudaFree(dev);
+                if (host) cudaFreeHost(host);
+                if (st) cudaStreamDestroy(st);
+                dev = host = nullptr;
+                dev_bytes = host_bytes = 0;
+                st = nullptr;
+                smem_set = false;
+        }
+        ~ThreadWork() { release(); }
+
+        // stream, dbytes on the device and hbytes pinned on the host
+        int reserve(size_t dbytes, size_t hbytes)
+        {
+                int d = 0;
+                T3NS_CUDA_TRY(cudaGetDevice(&d));
+                if (d != device) {
+                        release();
+                        device = d;
+                }
+                if (!st && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+                        st = nullptr;
+                        return set_error(T3NS_E_CUDA, "dense: stream creation failed");
+                }
+                if (dbytes > dev_bytes) {
+                        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
+                        const size_t want = std::max(dbytes, 2 * dev_bytes);
+                        if (dev) cudaFree(dev);
+                        dev = nullptr;
+                        dev_bytes = 0;
+                        if (cudaMalloc(&dev, want) != cudaSuccess) {
+                                cudaGetLastError();
+                                dev = nullptr;
+                                return set_error(T3NS_E_NOMEM, "dense: device workspace");
+                        }
+                        dev_bytes = want;
+                }
+                if (hbytes > host_bytes) {
+                        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
+                        const size_t want = std::max(hbytes, 2 * host_bytes);
+                        if (host) cudaFreeHost(host);
+                        host = nullptr;
+                        host_bytes = 0;
+                        if (cudaMallocHost(&host, want) != cudaSuccess) {
+                                cudaGetLastError();
+                                host = nullptr;
+                                return set_error(T3NS_E_NOMEM, "dense: pinned staging buffer");
+                        }
+                        host_bytes = want;
+                }
+                return T3NS_OK;
+        }
+};
+
+ThreadWork &thread_work()
 {
-        thread_local cudaStream_t s = nullptr;
-        if (!s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
-        return s;
+        thread_local ThreadWork w;
+        return w;
 }
 
-struct StreamAllocs {
-        cudaStream_t st;
-        std::vector<void *> v;
-        ~StreamAllocs()
-        {
-                for (void *p : v) cudaFreeAsync(p, st);
-        }
+// Byte offsets of consecutive arrays, each 256-byte aligned.
+struct Carve {
+        size_t off = 0;
         template <class T>
-        int get(T **p, size_t n)
+        size_t take(size_t n)
         {
-                void *q = nullptr;
-                if (cudaMallocAsync(&q, sizeof(T) * std::max<size_t>(n, 1), st) != cudaSuccess)
-                        return set_error(T3NS_E_NOMEM, "dense: device allocation failed");
-                v.push_back(q);
-                *p = static_cast<T *>(q);
-                return T3NS_OK;
+                const size_t at = off;
+                off += (sizeof(T) * std::max<size_t>(n, 1) + 255) & ~(size_t) 255;
+                return at;
         }
 };
 
@@ -364,60 +424,68 @@ int gesdd_run(char jobz, int m, int n, const double *a, int lda, double *s, doub
         const bool trans = m < n;
         const int mm = trans ? n : m, nn = k;
         const int vectors = jobz == 'S';
-        cudaStream_t st = thread_stream();
-        if (!st) return set_error(T3NS_E_CUDA, "gesdd: stream creation failed");
-        StreamAllocs al{st, {}};
-        double *dA, *W = nullptr, *V = nullptr;
-        SvdOut o;
-        int *status;
-        T3NS_TRY(al.get(&dA, (size_t) m * n));
-        T3NS_TRY(al.get(&o.sig, nn));
-        T3NS_TRY(al.get(&o.aux, nn));
-        T3NS_TRY(al.get(&o.rank, nn));
-        T3NS_TRY(al.get(&o.uw, vectors ? (size_t) mm * nn : 1));
-        T3NS_TRY(al.get(&o.vs, vectors ? (size_t) nn * nn : 1));
-        T3NS_TRY(al.get(&status, 1));
+        // device: A, then the outputs the host reads back (sigma, status and,
+        // with vectors, UW and VS) as one contiguous range, then the rest
         const size_t need = (size_t) mm * nn + (vectors ? (size_t) nn * nn : 0);
-        size_t smem = 0;
-        if (need <= (size_t) kSvdSmemDoubles) {
-                smem = need * sizeof(double);
-        } else {
-                T3NS_TRY(al.get(&W, (size_t) mm * nn));
-                T3NS_TRY(al.get(&V, vectors ? (size_t) nn * nn : 1));
-        }
-        std::vector<double> h((size_t) m * n);
-        pack(a, m, n, lda, h.data());
-        T3NS_CUDA_TRY(cudaMemcpyAsync(dA, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
-        T3NS_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
-        if (smem > 48 * 1024)
+        const bool in_smem = need <= (size_t) kSvdSmemDoubles;
+        Carve dc;
+        const size_t oA = dc.take<double>((size_t) m * n);
+        const size_t oSig = dc.take<double>(nn);
+        const size_t oStatus = dc.take<int>(1);
+        const size_t oUw = dc.take<double>(vectors ? (size_t) mm * nn : 1);
+        const size_t oVs = dc.take<double>(vectors ? (size_t) nn * nn : 1);
+        const size_t oEnd = dc.off;
+        const size_t oAux = dc.take<double>(nn);
+        const size_t oRank = dc.take<int>(nn);
+        const size_t oW = in_smem ? 0 : dc.take<double>((size_t) mm * nn);
+        const size_t oV = in_smem ? 0 : dc.take<double>(vectors ? (size_t) nn * nn : 1);
+        // host: packed A, then the copy of the output range
+        Carve hc;
+        const size_t hA = hc.take<double>((size_t) m * n);
+        const size_t hOut = hc.take<char>(oEnd - oSig);
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(tw.reserve(dc.off, hc.off));
+        cudaStream_t st = tw.st;
+        char *D = tw.dev, *H = tw.host;
+        SvdOut o;
+        o.sig = reinterpret_cast<double *>(D + oSig);
+        o.uw = reinterpret_cast<double *>(D + oUw);
+        o.vs = reinterpret_cast<double *>(D + oVs);
+        o.aux = reinterpret_cast<double *>(D + oAux);
+        o.rank = reinterpret_cast<int *>(D + oRank);
+        int *status = reinterpret_cast<int *>(D + oStatus);
+        double *dA = reinterpret_cast<double *>(D + oA);
+        double *W = in_smem ? nullptr : reinterpret_cast<double *>(D + oW);
+        double *V = in_smem ? nullptr : reinterpret_cast<double *>(D + oV);
+        const size_t smem = in_smem ? need * sizeof(double) : 0;
+        pack(a, m, n, lda, reinterpret_cast<double *>(H + hA));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(dA, H + hA, sizeof(double) * (size_t) m * n,
+                                      cudaMemcpyHostToDevice, st));
+        if (smem > 48 * 1024 && !tw.smem_set) {
                 T3NS_CUDA_TRY(cudaFuncSetAttribute(svd_jacobi_kernel,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    kSvdSmemDoubles * (int) sizeof(double)));
+                tw.smem_set = true;
+        }
         svd_jacobi_kernel<<<1, kDenseThreads, smem, st>>>(m, n, dA, W, V, vectors, o, status);
         T3NS_CUDA_TRY(cudaGetLastError());
-        int hstatus = 0;
-        T3NS_CUDA_TRY(cudaMemcpyAsync(s, o.sig, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
-        T3NS_CUDA_TRY(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, st));
-        std::vector<double> uw, vs;
-        if (vectors) {
-                uw.resize((size_t) mm * nn);
-                vs.resize((size_t) nn * nn);
-                T3NS_CUDA_TRY(cudaMemcpyAsync(uw.data(), o.uw, sizeof(double) * uw.size(),
-                                              cudaMemcpyDeviceToHost, st));
-                T3NS_CUDA_TRY(cudaMemcpyAsync(vs.data(), o.vs, sizeof(double) * vs.size(),
-                                              cudaMemcpyDeviceToHost, st));
-        }
+        T3NS_CUDA_TRY(cudaMemcpyAsync(H + hOut, D + oSig, oEnd - oSig, cudaMemcpyDeviceToHost, st));
         T3NS_CUDA_TRY(cudaStreamSynchronize(st));
+        const char *ho = H + hOut;
+        const int hstatus = *reinterpret_cast<const int *>(ho + (oStatus - oSig));
+        std::memcpy(s, ho, sizeof(double) * nn);
+        const double *uw = reinterpret_cast<const double *>(ho + (oUw - oSig));
+        const double *vs = reinterpret_cast<const double *>(ho + (oVs - oSig));
         if (hstatus) return set_error(T3NS_E_EIG, "gesdd: Jacobi sweeps did not converge");
         if (!vectors) return T3NS_OK;
         if (!trans) {
                 // A = UW S VS^T: U = UW (m x k), VT = VS^T (k x n)
-                unpack(uw.data(), m, k, u, ldu);
+                unpack(uw, m, k, u, ldu);
                 for (int j = 0; j < n; ++j)
                         for (int r = 0; r < k; ++r) vt[r + (int64_t) j * ldvt] = vs[j + (int64_t) r * nn];
         } else {
                 // A^T = UW S VS^T: U = VS (m x k), VT = UW^T (k x n)
-                unpack(vs.data(), m, k, u, ldu);
+                unpack(vs, m, k, u, ldu);
                 for (int j = 0; j < n; ++j)
                         for (int r = 0; r < k; ++r) vt[r + (int64_t) j * ldvt] = uw[j + (int64_t) r * mm];
         }
@@ -427,22 +495,23 @@ int gesdd_run(char jobz, int m, int n, const double *a, int lda, double *s, doub
 int geqrf_run(int m, int n, double *a, int lda, double *tau)
 {
         if (m < 0 || n < 0 || lda < std::max(1, m)) return set_error(T3NS_E_ARG, "geqrf: bad arguments");
-        if (std::min(m, n) == 0) return T3NS_OK;
-        cudaStream_t st = thread_stream();
-        if (!st) return set_error(T3NS_E_CUDA, "geqrf: stream creation failed");
-        StreamAllocs al{st, {}};
-        double *dA, *dT;
-        T3NS_TRY(al.get(&dA, (size_t) m * n));
-        T3NS_TRY(al.get(&dT, std::min(m, n)));
-        std::vector<double> h((size_t) m * n);
-        pack(a, m, n, lda, h.data());
-        T3NS_CUDA_TRY(cudaMemcpyAsync(dA, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
-        geqr2_kernel<<<1, kDenseThreads, 0, st>>>(m, n, dA, dT);
+        const int k = std::min(m, n);
+        if (k == 0) return T3NS_OK;
+        // device and host alike: A, then tau (read back together)
+        const size_t na = (size_t) m * n;
+        const size_t bytes = sizeof(double) * (na + k);
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(tw.reserve(bytes, bytes));
+        cudaStream_t st = tw.st;
+        double *dA = reinterpret_cast<double *>(tw.dev), *hA = reinterpret_cast<double *>(tw.host);
+        pack(a, m, n, lda, hA);
+        T3NS_CUDA_TRY(cudaMemcpyAsync(dA, hA, sizeof(double) * na, cudaMemcpyHostToDevice, st));
+        geqr2_kernel<<<1, kDenseThreads, 0, st>>>(m, n, dA, dA + na);
         T3NS_CUDA_TRY(cudaGetLastError());
-        T3NS_CUDA_TRY(cudaMemcpyAsync(h.data(), dA, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
-        T3NS_CUDA_TRY(cudaMemcpyAsync(tau, dT, sizeof(double) * std::min(m, n), cudaMemcpyDeviceToHost, st));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(hA, dA, bytes, cudaMemcpyDeviceToHost, st));
         T3NS_CUDA_TRY(cudaStreamSynchronize(st));
-        unpack(h.data(), m, n, a, lda);
+        unpack(hA, m, n, a, lda);
+        std::memcpy(tau, hA + na, sizeof(double) * k);
         return T3NS_OK;
 }
 
@@ -451,21 +520,21 @@ int orgqr_run(int m, int n, int k, double *a, int lda, const double *tau)
         if (m < 0 || n < 0 || n > m || k < 0 || k > n || lda < std::max(1, m))
                 return set_error(T3NS_E_ARG, "orgqr: bad arguments");
         if (n == 0) return T3NS_OK;
-        cudaStream_t st = thread_stream();
-        if (!st) return set_error(T3NS_E_CUDA, "orgqr: stream creation failed");
-        StreamAllocs al{st, {}};
-        double *dA, *dT;
-        T3NS_TRY(al.get(&dA, (size_t) m * n));
-        T3NS_TRY(al.get(&dT, k));
-        std::vector<double> h((size_t) m * n);
-        pack(a, m, n, lda, h.data());
-        T3NS_CUDA_TRY(cudaMemcpyAsync(dA, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
-        if (k) T3NS_CUDA_TRY(cudaMemcpyAsync(dT, tau, sizeof(double) * k, cudaMemcpyHostToDevice, st));
-        org2r_kernel<<<1, kDenseThreads, 0, st>>>(m, n, k, dA, dT);
+        // device and host alike: A, then tau (uploaded together)
+        const size_t na = (size_t) m * n;
+        const size_t bytes = sizeof(double) * (na + std::max(k, 1));
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(tw.reserve(bytes, bytes));
+        cudaStream_t st = tw.st;
+        double *dA = reinterpret_cast<double *>(tw.dev), *hA = reinterpret_cast<double *>(tw.host);
+        pack(a, m, n, lda, hA);
+        if (k) std::memcpy(hA + na, tau, sizeof(double) * k);
+        T3NS_CUDA_TRY(cudaMemcpyAsync(dA, hA, sizeof(double) * (na + k), cudaMemcpyHostToDevice, st));
+        org2r_kernel<<<1, kDenseThreads, 0, st>>>(m, n, k, dA, dA + na);
         T3NS_CUDA_TRY(cudaGetLastError());
-        T3NS_CUDA_TRY(cudaMemcpyAsync(h.data(), dA, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(hA, dA, sizeof(double) * na, cudaMemcpyDeviceToHost, st));
         T3NS_CUDA_TRY(cudaStreamSynchronize(st));
-        unpack(h.data(), m, n, a, lda);
+        unpack(hA, m, n, a, lda);
         return T3NS_OK;
 }
 

@@ -254,6 +254,45 @@ def test_qr_gpu_edge_cases(name):
     assert np.linalg.norm(q @ np.triu(qr)[:k] - a) <= 1e-13 * max(np.linalg.norm(a), 1e-300) * 10
 
 
+@pytest.mark.gpu
+def test_dense_workspace_reuse_across_sizes_and_threads():
+    """Each host thread keeps its device workspace and pinned staging buffer
+    between calls and grows them on demand: results of a call do not depend
+    on the sizes that ran before it on the thread, nor on other threads
+    calling at the same time (bit-identical to one call at a time)."""
+    import threading
+    names = sorted(EDGE)
+    order = names + names[::-1]        # sizes grow and shrink on one thread
+
+    def run(name):
+        a = EDGE[name]
+        u, s, vt = gpu_gesdd(a, "S")
+        qr, tau = gpu_geqrf(a)
+        k = min(a.shape)
+        return u, s, vt, qr, tau, gpu_orgqr(qr, tau, k, k)
+
+    alone = {name: run(name) for name in names}
+    for name in order:
+        for x, y in zip(run(name), alone[name]):
+            assert np.array_equal(x, y), name
+    errors = []
+
+    def worker(seed):
+        try:
+            for name in np.random.default_rng(seed).permutation(order):
+                for x, y in zip(run(name), alone[name]):
+                    assert np.array_equal(x, y), name
+        except Exception as e:          # reported on the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+
+
 def test_engine_declares_dense_entry_points():
     hdr = open(os.path.join(ROOT, "include", "t3ns_b200.h")).read()
     for name in ("t3ns_gesdd_host", "t3ns_geqrf_host", "t3ns_orgqr_host"):
