@@ -161,7 +161,11 @@ def run_engine(args, rank, world):
     sh = stream.cuda_stream
 
     peak = measure_fp64_peak(torch) if rank == 0 else None
-    tune_ms = plan.autotune(reps=2)        # the engine's autotuner picks the configuration
+    if args.kernel_config is None:
+        tune_ms = plan.autotune(reps=2)    # the engine's autotuner picks the configuration
+    else:
+        tune_ms = None
+        plan.set_config(args.kernel_config)
 
     for _ in range(args.warmup):
         plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
@@ -189,7 +193,11 @@ def run_engine(args, rank, world):
     from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_FP64
     y64 = y.clone()
     plan.set_precision(T3NS_PREC_3XTF32)
-    split_tune = plan.autotune(reps=1)
+    if args.split_kernel_config is None:
+        split_tune = plan.autotune(reps=1)
+    else:
+        split_tune = None
+        plan.set_config(args.split_kernel_config)
     for _ in range(args.warmup):
         plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
     torch.cuda.synchronize()
@@ -207,7 +215,10 @@ def run_engine(args, rank, world):
     split_err = float((y - y64).norm() / y64.norm())
     split_cfg = plan.config()
     plan.set_precision(T3NS_PREC_FP64)
-    plan.autotune(reps=1, force=False)
+    if args.kernel_config is None:
+        plan.autotune(reps=1, force=False)
+    else:
+        plan.set_config(args.kernel_config)
     y.copy_(y64)
 
     # e2e: host buffers (pinned) through the C-ABI host entry point
@@ -250,7 +261,7 @@ def run_engine(args, rank, world):
                    "autotune_ms": tune_ms},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
-                     "traffic": traffic_from_profile(path),
+                     "traffic": traffic_from_profile(path, plan.config()),
                      "peak_source": "measured this run: cuBLAS DGEMM 8192^3 via torch (FP64 "
                                     "peak; MEASURED_PEAKS.json has no FP64 figure)"},
         "e2e": {"value": flops * args.steps * world / t_e2e / 1e12, "unit": UNIT,
@@ -444,15 +455,18 @@ def serving_stream():
     return summary
 
 
-def traffic_from_profile(workload_path):
-    """DRAM bytes (read + write) of one FP64 heff_kernel launch (kernel
-    configuration 0) on this workload, from the ncu capture summarised under
-    profiles/ (None if that workload has not been profiled)."""
+def traffic_from_profile(workload_path, kernel_config):
+    """DRAM bytes (read + write) of one FP64 heff_kernel launch in kernel
+    configuration `kernel_config` on this workload, from the ncu capture
+    summarised under profiles/ (None if that workload and configuration have
+    not been profiled)."""
     p = os.path.join(ROOT, "profiles", "heff_kernel_traffic.json")
     if not os.path.exists(p):
         return None
     rec = json.load(open(p)).get(os.path.basename(workload_path))
-    return None if rec is None else rec["dram_bytes_per_launch"]
+    if rec is None or rec.get("kernel_config") != kernel_config:
+        return None
+    return rec["dram_bytes_per_launch"]
 
 
 def cpu_baseline(path, samples=1, stride=None, target_s=15.0):
@@ -492,6 +506,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default=None)
+    ap.add_argument("--kernel-config", type=int, default=None,
+                    help="run the FP64 matvec in this kernel configuration instead of the "
+                         "autotuner's choice (profiling: the autotuner's event timing is "
+                         "distorted under a profiler)")
+    ap.add_argument("--split-kernel-config", type=int, default=None,
+                    help="the same for the split-precision matvec")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true",
                     help="skip the whole-sweep FP64 vs split-precision comparison")

@@ -116,8 +116,10 @@ int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag);
 
 /* Kernel configurations of the matvec: 0 = one 512-thread CTA per SM with
  * large shared-memory output tiles, 1 = two 256-thread CTAs per SM with small
- * tiles.  Each has its own tiling of the plan (built on first use). */
-#define T3NS_NUM_CONFIGS 2
+ * tiles, 2 = one 768-thread CTA per SM (more warps, fewer registers a thread)
+ * with mid-size tiles.  Each has its own tiling of the plan (built on first
+ * use). */
+#define T3NS_NUM_CONFIGS 3
 int t3ns_heff_set_config(t3ns_heff *h, int config);
 int t3ns_heff_get_config(const t3ns_heff *h);
 

@@ -61,11 +61,19 @@ struct CfgSmall {
         static constexpr int kThreads = 256, kMinBlocks = 2;
         static constexpr int kOut = 3072, kPsi = 1024, kW = 9472;
 };
+// 24 warps per SM at 80 registers a thread: more warps to hide operand
+// latency on large steps, at the price of a few spilled registers
+struct CfgWide {
+        static constexpr int kThreads = 768, kMinBlocks = 1;
+        static constexpr int kOut = 6144, kPsi = 1024, kW = 19456;
+};
 const KernelCfg kCfgs[kNumCfgs] = {
         {CfgLarge::kThreads, CfgLarge::kMinBlocks, CfgLarge::kOut, CfgLarge::kPsi, CfgLarge::kW,
          "fp64-512x1-out8192"},
         {CfgSmall::kThreads, CfgSmall::kMinBlocks, CfgSmall::kOut, CfgSmall::kPsi, CfgSmall::kW,
          "fp64-256x2-out3072"},
+        {CfgWide::kThreads, CfgWide::kMinBlocks, CfgWide::kOut, CfgWide::kPsi, CfgWide::kW,
+         "fp64-768x1-out6144"},
 };
 
 
@@ -1294,14 +1302,18 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         if (dt.n_units == 0) return T3NS_OK;
         if (split) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
-        static_assert(kNumCfgs == 2, "one launch branch per configuration");
+        static_assert(kNumCfgs == 3, "one launch branch per configuration");
         int rc;
-        if (split)
-                rc = dp.active == 0 ? launch_cfg<CfgLarge, float2>(dp, dt, dp.x_split, dp.ops_split, y, s)
-                                    : launch_cfg<CfgSmall, float2>(dp, dt, dp.x_split, dp.ops_split, y, s);
-        else
-                rc = dp.active == 0 ? launch_cfg<CfgLarge, double>(dp, dt, x, dp.ops, y, s)
-                                    : launch_cfg<CfgSmall, double>(dp, dt, x, dp.ops, y, s);
+        if (split) {
+                const float2 *xs = dp.x_split, *os = dp.ops_split;
+                rc = dp.active == 0   ? launch_cfg<CfgLarge, float2>(dp, dt, xs, os, y, s)
+                     : dp.active == 1 ? launch_cfg<CfgSmall, float2>(dp, dt, xs, os, y, s)
+                                      : launch_cfg<CfgWide, float2>(dp, dt, xs, os, y, s);
+        } else {
+                rc = dp.active == 0   ? launch_cfg<CfgLarge, double>(dp, dt, x, dp.ops, y, s)
+                     : dp.active == 1 ? launch_cfg<CfgSmall, double>(dp, dt, x, dp.ops, y, s)
+                                      : launch_cfg<CfgWide, double>(dp, dt, x, dp.ops, y, s);
+        }
         T3NS_TRY(rc);
         if (launches) *launches = split ? 2 : 1;
         return T3NS_OK;

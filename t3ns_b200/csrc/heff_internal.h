@@ -52,7 +52,7 @@ struct KernelCfg {
         int w_cap;         // intermediates of a group of terms
         const char *name;
 };
-constexpr int kNumCfgs = 2;
+constexpr int kNumCfgs = 3;
 extern const KernelCfg kCfgs[kNumCfgs];
 
 // One (new, old) pair before tiling: its terms and the old block's dims.

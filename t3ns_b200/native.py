@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(_HERE, "_lib")
 
 T3NS_PREC_FP64 = 0
-T3NS_NUM_CONFIGS = 2   # kernel configurations of the matvec
+T3NS_NUM_CONFIGS = 3   # kernel configurations of the matvec
 T3NS_PREC_3XTF32 = 1
 T3NS_PREC_BF16X3 = 2
 
