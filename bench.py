@@ -365,12 +365,25 @@ def other_rows_measurement(reps=3):
     call), on every captured call of the Hubbard and 12-orbital QC sweeps:
     algorithmic GFLOP and GPU seconds (best of `reps` per call); the SVDs
     also timed through the reference's LAPACK (OpenBLAS LAPACKE_dgesdd) on the
-    host for comparison.  None if the captures are absent."""
+    host for comparison, one call at a time and all calls from a pool of host
+    threads (the reference decomposes a split's sectors in an OpenMP loop,
+    src/siteTensor_decompose.c:1413).  None if the captures are absent."""
     import ctypes as C
     from t3ns_b200 import native, updates
     from t3ns_b200.stepfile import read_step
     caps = os.path.join(ROOT, "oracle", "_ref", "captures")
     out = {}
+
+    def bound_call(fn, a_in, jobz, m, n):
+        """One SVD call with its own input copy and output arrays."""
+        k = min(m, n)
+        s_, u, vt = np.zeros(k), np.zeros(max(m * k, 1)), np.zeros(max(k * n, 1))
+
+        def go():
+            a = np.array(a_in)
+            fn(jobz.encode(), m, n, a.ctypes.data, m, s_.ctypes.data, u.ctypes.data, m,
+               vt.ctypes.data, k)
+        return go
 
     def best(fn):
         t = []
@@ -413,6 +426,7 @@ def other_rows_measurement(reps=3):
     files = sorted(glob.glob(os.path.join(caps, "dense_*", "gesdd_*.t3c")))
     gpu_s = cpu_s = 0.0
     largest = (0, 0)
+    pool_calls = []          # (GPU call, LAPACK call), each with its own arrays
     for f in files:
         r = read_step(f)
         m, n = int(r["gesdd.m"][0]), int(r["gesdd.n"][0])
@@ -421,21 +435,27 @@ def other_rows_measurement(reps=3):
         if k == 0:
             continue
         largest = max(largest, (m, n), key=lambda x: x[0] * x[1])
-        s_ = np.zeros(k)
-        u = np.zeros(max(m * k, 1))
-        vt = np.zeros(max(k * n, 1))
+        gpu_call = bound_call(lambda *x: native.check(lib.t3ns_gesdd_host(*x), "gesdd"),
+                              r["gesdd.a"], jobz, m, n)
+        cpu_call = bound_call(lambda *x: cpu.LAPACKE_dgesdd(102, *x), r["gesdd.a"], jobz, m, n) \
+            if cpu is not None else None
+        gpu_s += best(gpu_call)
+        if cpu_call is not None:
+            cpu_s += best(cpu_call)
+        pool_calls.append((gpu_call, cpu_call))
 
-        def run(fn):
-            def go():
-                a = np.array(r["gesdd.a"])
-                fn(jobz.encode(), m, n, a.ctypes.data, m, s_.ctypes.data, u.ctypes.data, m,
-                   vt.ctypes.data, k)
-            return go
-        gpu_s += best(run(lambda *x: native.check(lib.t3ns_gesdd_host(*x), "gesdd")))
-        if cpu is not None:
-            cpu_s += best(run(lambda *x: cpu.LAPACKE_dgesdd(102, *x)))
+    from concurrent.futures import ThreadPoolExecutor
+    workers = min(16, os.cpu_count() or 1)
+
+    def pooled(fns):
+        with ThreadPoolExecutor(workers) as ex:
+            return best(lambda: list(ex.map(lambda fn: fn(), fns)))
     out["gesdd"] = {"calls": len(files), "largest": list(largest), "gpu_seconds_e2e": gpu_s,
-                    "reference_lapack_seconds": cpu_s if cpu is not None else None}
+                    "reference_lapack_seconds": cpu_s if cpu is not None else None,
+                    "host_threads": workers,
+                    "gpu_seconds_e2e_threads": pooled([g for g, _ in pool_calls]),
+                    "reference_lapack_seconds_threads":
+                        pooled([c for _, c in pool_calls]) if cpu is not None else None}
     return out
 
 
