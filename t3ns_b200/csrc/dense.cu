@@ -4,9 +4,8 @@
 // LAPACKE_dgeqrf at :285, LAPACKE_dorgqr at :295), one symmetry sector per
 // call.  Each call runs as one CTA on the caller thread's own stream, so the
 // reference's OpenMP loop over sectors keeps several sectors in flight, and
-// costs one upload, one launch, one download and one synchronisation: the
-// thread's device workspace and pinned staging buffer are kept between
-// calls and only grow.
+// costs one upload, one launch, one download and one synchronisation through
+// the thread's workspace (thread_work.h).
 //
 // SVD: one-sided (Hestenes) Jacobi on the columns of the tall orientation W
 // of A (A or A^T), parallel round-robin ordering, rotations accumulated into
@@ -27,6 +26,7 @@
 #include <vector>
 
 #include "common.h"
+#include "thread_work.h"
 
 namespace t3ns {
 namespace {
@@ -315,90 +315,6 @@ org2r_kernel(int m, int n, int k, double *A, const double *__restrict__ tau)
         }
 }
 
-// Per host thread: the stream its calls run on, a device workspace and a
-// pinned host staging buffer, both kept between calls and grown (to at least
-// twice their size) when a call needs more.  Freed when the thread exits.
-struct ThreadWork {
-        int device = -1;
-        cudaStream_t st = nullptr;
-        char *dev = nullptr, *host = nullptr;
-        size_t dev_bytes = 0, host_bytes = 0;
-        bool smem_set = false;   // large dynamic shared memory enabled for the SVD
-
-        void release()
-        {
-                if (st) cudaStreamSynchronize(st);
-                if (dev) cudaFree(dev);
-                if (host) cudaFreeHost(host);
-                if (st) cudaStreamDestroy(st);
-                dev = host = nullptr;
-                dev_bytes = host_bytes = 0;
-                st = nullptr;
-                smem_set = false;
-        }
-        ~ThreadWork() { release(); }
-
-        // stream, dbytes on the device and hbytes pinned on the host
-        int reserve(size_t dbytes, size_t hbytes)
-        {
-                int d = 0;
-                T3NS_CUDA_TRY(cudaGetDevice(&d));
-                if (d != device) {
-                        release();
-                        device = d;
-                }
-                if (!st && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
-                        st = nullptr;
-                        return set_error(T3NS_E_CUDA, "dense: stream creation failed");
-                }
-                if (dbytes > dev_bytes) {
-                        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
-                        const size_t want = std::max(dbytes, 2 * dev_bytes);
-                        if (dev) cudaFree(dev);
-                        dev = nullptr;
-                        dev_bytes = 0;
-                        if (cudaMalloc(&dev, want) != cudaSuccess) {
-                                cudaGetLastError();
-                                dev = nullptr;
-                                return set_error(T3NS_E_NOMEM, "dense: device workspace");
-                        }
-                        dev_bytes = want;
-                }
-                if (hbytes > host_bytes) {
-                        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
-                        const size_t want = std::max(hbytes, 2 * host_bytes);
-                        if (host) cudaFreeHost(host);
-                        host = nullptr;
-                        host_bytes = 0;
-                        if (cudaMallocHost(&host, want) != cudaSuccess) {
-                                cudaGetLastError();
-                                host = nullptr;
-                                return set_error(T3NS_E_NOMEM, "dense: pinned staging buffer");
-                        }
-                        host_bytes = want;
-                }
-                return T3NS_OK;
-        }
-};
-
-ThreadWork &thread_work()
-{
-        thread_local ThreadWork w;
-        return w;
-}
-
-// Byte offsets of consecutive arrays, each 256-byte aligned.
-struct Carve {
-        size_t off = 0;
-        template <class T>
-        size_t take(size_t n)
-        {
-                const size_t at = off;
-                off += (sizeof(T) * std::max<size_t>(n, 1) + 255) & ~(size_t) 255;
-                return at;
-        }
-};
-
 // column-major m x n with leading dimension ld <-> compact
 void pack(const double *a, int m, int n, int64_t ld, double *c)
 {
@@ -461,11 +377,11 @@ int gesdd_run(char jobz, int m, int n, const double *a, int lda, double *s, doub
         pack(a, m, n, lda, reinterpret_cast<double *>(H + hA));
         T3NS_CUDA_TRY(cudaMemcpyAsync(dA, H + hA, sizeof(double) * (size_t) m * n,
                                       cudaMemcpyHostToDevice, st));
-        if (smem > 48 * 1024 && !tw.smem_set) {
+        if (smem > 48 * 1024 && !tw.svd_smem_set) {
                 T3NS_CUDA_TRY(cudaFuncSetAttribute(svd_jacobi_kernel,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    kSvdSmemDoubles * (int) sizeof(double)));
-                tw.smem_set = true;
+                tw.svd_smem_set = true;
         }
         svd_jacobi_kernel<<<1, kDenseThreads, smem, st>>>(m, n, dA, W, V, vectors, o, status);
         T3NS_CUDA_TRY(cudaGetLastError());

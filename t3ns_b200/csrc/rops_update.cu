@@ -22,11 +22,13 @@
 // to a per-CTA scratch slice, the second accumulates into the output; both
 // run on the FP64 tensor pipe (cta_dgemm).
 #include <algorithm>
+#include <cstring>
 #include <string>
 #include <vector>
 
 #include "common.h"
 #include "dmma_gemm.cuh"
+#include "thread_work.h"
 
 namespace t3ns {
 namespace {
@@ -170,24 +172,57 @@ bupdate_kernel(int3 ax, int nunits, const int *__restrict__ unit_ptr,
         }
 }
 
-template <class T>
-int upload(std::vector<void *> &allocs, T **p, const T *src, size_t n)
-{
-        *p = nullptr;
-        cudaError_t e = cudaMalloc((void **) p, sizeof(T) * std::max<size_t>(n, 1));
-        if (e != cudaSuccess) {
-                cudaGetLastError();
-                return set_error(T3NS_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+// The arrays of one call laid out in the thread's workspace: inputs first
+// (staged in the pinned buffer at their device offsets and uploaded with one
+// copy), then the zero-initialised outputs, then the scratch.
+struct CallLayout {
+        Carve c;
+        struct Input {
+                size_t off;
+                const void *src;
+                size_t bytes;
+        };
+        std::vector<Input> inputs;
+        template <class T>
+        size_t input(const T *src, size_t n)
+        {
+                const size_t o = c.take<T>(n);
+                inputs.push_back({o, src, src ? sizeof(T) * n : 0});
+                return o;
         }
-        allocs.push_back(*p);
-        if (src && n) T3NS_CUDA_TRY(cudaMemcpy(*p, src, sizeof(T) * n, cudaMemcpyHostToDevice));
+};
+
+// Stages and uploads the inputs (all placed before `in_end`) and zeroes
+// [zero0, zero1) on the device; `host_extra` more pinned bytes are reserved
+// for the download.
+int stage_call(ThreadWork &tw, const CallLayout &L, size_t in_end, size_t zero0, size_t zero1,
+               size_t host_extra)
+{
+        T3NS_TRY(tw.reserve(L.c.off, std::max(in_end, host_extra)));
+        for (const auto &x : L.inputs)
+                if (x.bytes) std::memcpy(tw.host + x.off, x.src, x.bytes);
+        T3NS_CUDA_TRY(cudaMemcpyAsync(tw.dev, tw.host, in_end, cudaMemcpyHostToDevice, tw.st));
+        if (zero1 > zero0) T3NS_CUDA_TRY(cudaMemsetAsync(tw.dev + zero0, 0, zero1 - zero0, tw.st));
         return T3NS_OK;
 }
 
-struct Allocs {
-        std::vector<void *> v;
-        ~Allocs() { for (void *p : v) cudaFree(p); }
-};
+// Downloads `bytes` from device offset `off` into dst (through the pinned
+// buffer) and waits for the call's stream.
+int finish_call(ThreadWork &tw, size_t off, void *dst, size_t bytes)
+{
+        if (bytes)
+                T3NS_CUDA_TRY(cudaMemcpyAsync(tw.host, tw.dev + off, bytes, cudaMemcpyDeviceToHost,
+                                              tw.st));
+        T3NS_CUDA_TRY(cudaStreamSynchronize(tw.st));
+        if (bytes) std::memcpy(dst, tw.host, bytes);
+        return T3NS_OK;
+}
+
+template <class T>
+T *at(const ThreadWork &tw, size_t off)
+{
+        return reinterpret_cast<T *>(tw.dev + off);
+}
 
 }  // namespace
 
@@ -217,43 +252,40 @@ int pupdate_run(const t3ns_pupdate_desc *d, const double *t_tel, const double *o
         for (int u = 0; u < d->nunits; ++u)
                 if (d->unit_ptr[u] > d->unit_ptr[u + 1] || d->unit_ptr[u + 1] > d->nentries)
                         return set_error(T3NS_E_ARG, "pupdate: unit list out of range");
-        Allocs a;
-        int *unit_ptr, *op_ptr, *counter;
-        int4 *dims;
-        int64_t *t_off, *ta_off, *old_off, *new_off;
-        double *pref, *T, *OLD, *NEW, *scratch;
-        std::vector<int4> dv(d->nentries);
-        for (int e = 0; e < d->nentries; ++e)
-                dv[e] = make_int4(d->dims[4 * e], d->dims[4 * e + 1], d->dims[4 * e + 2], d->dims[4 * e + 3]);
-        T3NS_TRY(upload(a.v, &unit_ptr, d->unit_ptr, d->nunits + 1));
-        T3NS_TRY(upload(a.v, &op_ptr, d->op_ptr, d->nentries + 1));
-        T3NS_TRY(upload(a.v, &dims, dv.data(), dv.size()));
-        T3NS_TRY(upload(a.v, &t_off, d->t_off, d->nentries));
-        T3NS_TRY(upload(a.v, &ta_off, d->ta_off, d->nentries));
-        T3NS_TRY(upload(a.v, &pref, d->pref, d->nentries));
-        T3NS_TRY(upload(a.v, &old_off, d->old_off, npairs));
-        T3NS_TRY(upload(a.v, &new_off, d->new_off, npairs));
-        T3NS_TRY(upload(a.v, &T, t_tel, d->t_elems));
-        T3NS_TRY(upload(a.v, &OLD, old_tel, d->old_elems));
-        T3NS_TRY(upload<double>(a.v, &NEW, nullptr, d->new_elems));
-        T3NS_TRY(upload<int>(a.v, &counter, nullptr, 1));
         int dev = 0, sms = 148;
         T3NS_CUDA_TRY(cudaGetDevice(&dev));
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const int grid = std::max(1, std::min(d->nunits, 4 * sms));
-        T3NS_TRY(upload<double>(a.v, &scratch, nullptr, (size_t) grid * slot));
-        T3NS_CUDA_TRY(cudaMemset(NEW, 0, sizeof(double) * std::max<int64_t>(d->new_elems, 1)));
-        T3NS_CUDA_TRY(cudaMemset(counter, 0, sizeof(int)));
+        CallLayout L;
+        const size_t o_unit = L.input(d->unit_ptr, d->nunits + 1);
+        const size_t o_op = L.input(d->op_ptr, d->nentries + 1);
+        // dims: four ints per entry, the layout of int4
+        const size_t o_dims = L.input(reinterpret_cast<const int4 *>(d->dims), d->nentries);
+        const size_t o_t = L.input(d->t_off, d->nentries);
+        const size_t o_ta = L.input(d->ta_off, d->nentries);
+        const size_t o_pref = L.input(d->pref, d->nentries);
+        const size_t o_old_off = L.input(d->old_off, npairs);
+        const size_t o_new_off = L.input(d->new_off, npairs);
+        const size_t o_T = L.input(t_tel, d->t_elems);
+        const size_t o_OLD = L.input(old_tel, d->old_elems);
+        const size_t in_end = L.c.off;
+        const size_t o_NEW = L.c.take<double>(d->new_elems);
+        const size_t o_counter = L.c.take<int>(1);
+        const size_t zero_end = L.c.off;
+        const size_t o_scratch = L.c.take<double>((size_t) grid * slot);
+        const size_t new_bytes = sizeof(double) * d->new_elems;
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(stage_call(tw, L, in_end, o_NEW, zero_end, new_bytes));
         if (d->nunits > 0) {
-                pupdate_kernel<<<grid, kUpdThreads>>>(d->is_left, d->nunits, unit_ptr, dims, t_off,
-                                                      ta_off, pref, op_ptr, old_off, new_off, T, OLD,
-                                                      NEW, scratch, slot, counter);
+                pupdate_kernel<<<grid, kUpdThreads, 0, tw.st>>>(
+                        d->is_left, d->nunits, at<int>(tw, o_unit), at<int4>(tw, o_dims),
+                        at<int64_t>(tw, o_t), at<int64_t>(tw, o_ta), at<double>(tw, o_pref),
+                        at<int>(tw, o_op), at<int64_t>(tw, o_old_off), at<int64_t>(tw, o_new_off),
+                        at<double>(tw, o_T), at<double>(tw, o_OLD), at<double>(tw, o_NEW),
+                        at<double>(tw, o_scratch), slot, at<int>(tw, o_counter));
                 T3NS_CUDA_TRY(cudaGetLastError());
         }
-        if (d->new_elems)
-                T3NS_CUDA_TRY(cudaMemcpy(new_tel, NEW, sizeof(double) * d->new_elems,
-                                         cudaMemcpyDeviceToHost));
-        return T3NS_OK;
+        return finish_call(tw, o_NEW, new_tel, new_bytes);
 }
 
 int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst)
@@ -263,25 +295,25 @@ int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst)
                 if (d->len[e] < 0 || d->src_off[e] < 0 || d->src_off[e] + d->len[e] > d->src_elems ||
                     d->dst_off[e] < 0 || d->dst_off[e] + d->len[e] > d->dst_elems)
                         return set_error(T3NS_E_ARG, "scalecopy: block out of range");
-        Allocs a;
-        int64_t *dst_off, *src_off;
-        int *len;
-        double *scale, *S, *D;
-        T3NS_TRY(upload(a.v, &dst_off, d->dst_off, d->nentries));
-        T3NS_TRY(upload(a.v, &src_off, d->src_off, d->nentries));
-        T3NS_TRY(upload(a.v, &len, d->len, d->nentries));
-        T3NS_TRY(upload(a.v, &scale, d->scale, d->nentries));
-        T3NS_TRY(upload(a.v, &S, src, d->src_elems));
-        T3NS_TRY(upload<double>(a.v, &D, nullptr, d->dst_elems));
-        T3NS_CUDA_TRY(cudaMemset(D, 0, sizeof(double) * std::max<int64_t>(d->dst_elems, 1)));
+        CallLayout L;
+        const size_t o_dst_off = L.input(d->dst_off, d->nentries);
+        const size_t o_src_off = L.input(d->src_off, d->nentries);
+        const size_t o_len = L.input(d->len, d->nentries);
+        const size_t o_scale = L.input(d->scale, d->nentries);
+        const size_t o_S = L.input(src, d->src_elems);
+        const size_t in_end = L.c.off;
+        const size_t o_D = L.c.take<double>(d->dst_elems);
+        const size_t dst_bytes = sizeof(double) * d->dst_elems;
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(stage_call(tw, L, in_end, o_D, L.c.off, dst_bytes));
         if (d->nentries > 0) {
-                scalecopy_kernel<<<std::min(d->nentries, 148 * 16), 256>>>(
-                        d->nentries, dst_off, src_off, len, scale, S, D);
+                scalecopy_kernel<<<std::min(d->nentries, 148 * 16), 256, 0, tw.st>>>(
+                        d->nentries, at<int64_t>(tw, o_dst_off), at<int64_t>(tw, o_src_off),
+                        at<int>(tw, o_len), at<double>(tw, o_scale), at<double>(tw, o_S),
+                        at<double>(tw, o_D));
                 T3NS_CUDA_TRY(cudaGetLastError());
         }
-        if (d->dst_elems)
-                T3NS_CUDA_TRY(cudaMemcpy(dst, D, sizeof(double) * d->dst_elems, cudaMemcpyDeviceToHost));
-        return T3NS_OK;
+        return finish_call(tw, o_D, dst, dst_bytes);
 }
 
 int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o1_tel,
@@ -322,42 +354,42 @@ int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o
                         return set_error(T3NS_E_ARG, "bupdate: unit list out of range");
         w1cap = (w1cap + 31) / 32 * 32;
         w2cap = (w2cap + 31) / 32 * 32;
-        Allocs al;
-        int *unit_ptr, *op_ptr, *dims, *counter;
-        int64_t *t_off, *ta_off, *o1_off, *o2_off, *new_off;
-        double *pref, *T, *O1, *O2, *NEW, *scratch;
-        T3NS_TRY(upload(al.v, &unit_ptr, d->unit_ptr, d->nunits + 1));
-        T3NS_TRY(upload(al.v, &op_ptr, d->op_ptr, d->nentries + 1));
-        T3NS_TRY(upload(al.v, &dims, d->dims, (size_t) 6 * d->nentries));
-        T3NS_TRY(upload(al.v, &t_off, d->t_off, d->nentries));
-        T3NS_TRY(upload(al.v, &ta_off, d->ta_off, d->nentries));
-        T3NS_TRY(upload(al.v, &pref, d->pref, d->nentries));
-        T3NS_TRY(upload(al.v, &o1_off, d->o1_off, ntr));
-        T3NS_TRY(upload(al.v, &o2_off, d->o2_off, ntr));
-        T3NS_TRY(upload(al.v, &new_off, d->new_off, ntr));
-        T3NS_TRY(upload(al.v, &T, t_tel, d->t_elems));
-        T3NS_TRY(upload(al.v, &O1, o1_tel, d->o1_elems));
-        T3NS_TRY(upload(al.v, &O2, o2_tel, d->o2_elems));
-        T3NS_TRY(upload<double>(al.v, &NEW, nullptr, d->new_elems));
-        T3NS_TRY(upload<int>(al.v, &counter, nullptr, 1));
         int dev = 0, sms = 148;
         T3NS_CUDA_TRY(cudaGetDevice(&dev));
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const int grid = std::max(1, std::min(d->nunits, 4 * sms));
-        T3NS_TRY(upload<double>(al.v, &scratch, nullptr, (size_t) grid * (w1cap + w2cap)));
-        T3NS_CUDA_TRY(cudaMemset(NEW, 0, sizeof(double) * std::max<int64_t>(d->new_elems, 1)));
-        T3NS_CUDA_TRY(cudaMemset(counter, 0, sizeof(int)));
+        CallLayout L;
+        const size_t o_unit = L.input(d->unit_ptr, d->nunits + 1);
+        const size_t o_op = L.input(d->op_ptr, d->nentries + 1);
+        const size_t o_dims = L.input(d->dims, (size_t) 6 * d->nentries);
+        const size_t o_t = L.input(d->t_off, d->nentries);
+        const size_t o_ta = L.input(d->ta_off, d->nentries);
+        const size_t o_pref = L.input(d->pref, d->nentries);
+        const size_t o_o1_off = L.input(d->o1_off, ntr);
+        const size_t o_o2_off = L.input(d->o2_off, ntr);
+        const size_t o_new_off = L.input(d->new_off, ntr);
+        const size_t o_T = L.input(t_tel, d->t_elems);
+        const size_t o_O1 = L.input(o1_tel, d->o1_elems);
+        const size_t o_O2 = L.input(o2_tel, d->o2_elems);
+        const size_t in_end = L.c.off;
+        const size_t o_NEW = L.c.take<double>(d->new_elems);
+        const size_t o_counter = L.c.take<int>(1);
+        const size_t zero_end = L.c.off;
+        const size_t o_scratch = L.c.take<double>((size_t) grid * (w1cap + w2cap));
+        const size_t new_bytes = sizeof(double) * d->new_elems;
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(stage_call(tw, L, in_end, o_NEW, zero_end, new_bytes));
         if (d->nunits > 0) {
-                bupdate_kernel<<<grid, kUpdThreads>>>(make_int3(a, b, g), d->nunits, unit_ptr, dims,
-                                                      t_off, ta_off, pref, op_ptr, o1_off, o2_off,
-                                                      new_off, T, O1, O2, NEW, scratch, w1cap, w2cap,
-                                                      counter);
+                bupdate_kernel<<<grid, kUpdThreads, 0, tw.st>>>(
+                        make_int3(a, b, g), d->nunits, at<int>(tw, o_unit), at<int>(tw, o_dims),
+                        at<int64_t>(tw, o_t), at<int64_t>(tw, o_ta), at<double>(tw, o_pref),
+                        at<int>(tw, o_op), at<int64_t>(tw, o_o1_off), at<int64_t>(tw, o_o2_off),
+                        at<int64_t>(tw, o_new_off), at<double>(tw, o_T), at<double>(tw, o_O1),
+                        at<double>(tw, o_O2), at<double>(tw, o_NEW), at<double>(tw, o_scratch), w1cap,
+                        w2cap, at<int>(tw, o_counter));
                 T3NS_CUDA_TRY(cudaGetLastError());
         }
-        if (d->new_elems)
-                T3NS_CUDA_TRY(cudaMemcpy(new_tel, NEW, sizeof(double) * d->new_elems,
-                                         cudaMemcpyDeviceToHost));
-        return T3NS_OK;
+        return finish_call(tw, o_NEW, new_tel, new_bytes);
 }
 
 }  // namespace t3ns

@@ -41,3 +41,20 @@ def test_pupdate_gpu_matches_reference(path):
         pytest.skip("no CUDA device")
     rec, sch = _load(path)
     assert rc.kick_and_compare(rec, sch, rc.run_pupdate_gpu(rec, sch)) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not CAPS, reason="no update captures")
+def test_pupdate_workspace_reuse_is_exact():
+    """The host calls stage through a per-thread workspace that keeps the
+    largest call's buffers: every call gives the same bits whatever ran
+    before it on the thread (calls in both size orders), so no output of an
+    earlier call leaks into a later one."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    loaded = [_load(p) for p in CAPS]
+    order = sorted(range(len(loaded)), key=lambda i: loaded[i][0]["T.tel"].size)
+    first = {i: rc.run_pupdate_gpu(*loaded[i]) for i in order[::-1]}     # largest first
+    for i in order:                                                      # then smallest first
+        assert np.array_equal(rc.run_pupdate_gpu(*loaded[i]), first[i]), CAPS[i]
