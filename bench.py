@@ -137,6 +137,17 @@ def measure_fp64_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
+def max_over_ranks(values, world, device):
+    """Each value's maximum over the ranks (the slowest rank's time); the
+    values unchanged on one rank.  A collective: every rank calls it."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def run_engine(args, rank, world):
     import torch
 
@@ -239,10 +250,8 @@ def run_engine(args, rank, world):
     err = float((yh.cuda() - y).norm() / y.norm())
     assert err < 1e-12, err
 
-    if world > 1:
-        tt = torch.tensor([t_total, t_e2e], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_total, t_e2e = float(tt[0]), float(tt[1])
+    # every rank takes this collective, in the same order
+    t_total, t_e2e, t_split = max_over_ranks([t_total, t_e2e, t_split], world, "cuda")
     if rank != 0:
         return None
     flops = st["flops_ref"]
@@ -577,6 +586,10 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     out = run_engine(args, rank, world)
+    if world > 1:
+        # the CPU baseline, Davidson, sweep, serving and update figures are
+        # single-GPU measurements, taken at N=1 only
+        args.no_cpu_baseline = args.no_sweep = args.no_serving = True
     if rank == 0:
         if not args.no_cpu_baseline:
             cb = cpu_baseline(pick_workload(args.workload), samples=1)
