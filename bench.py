@@ -34,6 +34,7 @@ import os
 import re
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -42,6 +43,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Heff TFLOP/s"
+WORKLOAD_NAME = ("synthetic QC 24 orbitals, 24 e-, U1xSU2, D=512, SITE_SIZE 2: "
+                 "one step's Heff matvec")
 UNIT = "TFLOP/s"
 DEFAULT_WORKLOAD_DIR = os.path.join(ROOT, "oracle", "_ref", "workloads")
 
@@ -75,11 +78,11 @@ class Clocks:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="t3ns_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
@@ -99,7 +102,10 @@ class Clocks:
         if not self.proc:
             return None
         rows = []
-        for line in open(self.path):
+        with open(self.path) as f:
+            lines = f.readlines()
+        os.unlink(self.path)
+        for line in lines:
             p = [x.strip() for x in line.split(",")]
             if len(p) >= 9:
                 rows.append(p)
@@ -262,8 +268,7 @@ def run_engine(args, rank, world):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "synthetic QC 24 orbitals, 24 e-, U1xSU2, D=512, SITE_SIZE 2: "
-                               "one step's Heff matvec (" + os.path.basename(path) + ")",
+        "config": {"workload": WORKLOAD_NAME + " (" + os.path.basename(path) + ")",
                    **step_stats(s), "flops_per_matvec": flops,
                    "parallelism": f"replicas{world}", "l2": "flushed between iterations",
                    "precision": "fp64", "kernel_config": plan.config(),
@@ -300,7 +305,8 @@ def sweep_comparison(timeout=900):
         return None
     from t3ns_b200.workloads import synthetic_qc_fcidump
     net = os.path.join(ROOT, "tests", "golden", "networks")
-    fcid = synthetic_qc_fcidump(os.path.join("/tmp", "t3ns_bench_qc12.FCIDUMP"), 12, 12, 0, 72)
+    tmp = tempfile.mkdtemp(prefix="t3ns_bench_")
+    fcid = synthetic_qc_fcidump(os.path.join(tmp, "qc12.FCIDUMP"), 12, 12, 0, 72)
     cases = {
         "hubbard10_D128_6sweeps": ["--net", os.path.join(net, "t3ns_10.netw"), "--inter",
                                    "NN_HUBBARD ( t = 1 U = 4 )", "--symm", "Z2,U1,SU2", "--ts",
@@ -565,16 +571,26 @@ def main():
             return
         flops = res["flops"]
         v = flops / res["seconds_per_matvec"] / 1e12
+        sample = (f"{res['calls']} calls (median taken) of the reference matvecT3NS "
+                  f"(exec_secondrun) restricted to every {res['stride']}-th output block of "
+                  f"this step ({res['sampled_blocks']} of {res['blocks']} blocks, "
+                  f"{flops / res['flops_full']:.3f} of the full matvec's FLOPs); the full "
+                  f"matvec's time is estimated at this rate")
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
+            "steps": res["calls"], "warmup": 0,
             "ms_per_step": 1e3 * res["seconds_per_matvec"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": os.path.basename(path), **step_stats(s)},
+            "config": {"workload": WORKLOAD_NAME + " (" + os.path.basename(path) + ")",
+                       **step_stats(s), "flops_per_matvec": res["flops_full"],
+                       "parallelism": f"replicas{world}", "precision": "fp64"},
+            "sample": {"stride": res["stride"], "calls": res["calls"],
+                       "flops_per_call": flops, "flops_full_matvec": res["flops_full"],
+                       "ms_per_call": 1e3 * res["seconds_per_matvec"],
+                       "ms_per_full_matvec_est": 1e3 * res["seconds_per_matvec"] *
+                       res["flops_full"] / flops},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": res["cores"], "kind": "reference",
-                             "sample": f"{res['calls']} calls of the reference matvecT3NS "
-                                       f"(exec_secondrun) on every {res['stride']}-th output "
-                                       "block of this step"},
+                             "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
         return

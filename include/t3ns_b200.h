@@ -106,8 +106,16 @@ int t3ns_heff_create(const t3ns_heff_desc *desc, int precision, t3ns_heff **out)
  * Replaces exec_secondrun (reference src/Heff.c:945-1000). */
 int t3ns_heff_matvec_device(t3ns_heff *h, const double *x, double *y, void *stream);
 
-/* Same with host buffers: x is copied to the device, y back to the host. */
+/* Same with host buffers: x is copied to the device, y back to the host.
+ * Synchronises and returns T3NS_E_DEVICE if the kernel reported an error. */
 int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y);
+
+/* Error status of the matvecs enqueued so far on `stream`: waits for the
+ * stream, returns T3NS_E_DEVICE (and clears the status) if a matvec kernel
+ * reported an error, else T3NS_OK.  t3ns_heff_matvec_device is asynchronous
+ * and does not wait; callers of the device entry point check here (the
+ * device Davidson checks after every iteration by itself). */
+int t3ns_heff_check_status(t3ns_heff *h, void *stream);
 
 /* Diagonal of Heff into a device (or host) buffer of size doubles.
  * Replaces make_diagonal (reference src/Heff.c:1268-1312). */

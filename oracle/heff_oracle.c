@@ -63,15 +63,14 @@ static const double *op_block(const t3ns_ropset *rs, int op, int sb, int *sz)
         return rs->op_tel[op] + bb[sb];
 }
 
-int t3ns_oracle_matvec(const t3ns_heff_desc *d, const double *x, double *y)
+/* Accumulates new block nb of the matvec into y (zeroed by the caller). */
+static void matvec_block(const t3ns_heff_desc *d, const double *x, double *y, int nb)
 {
         const int nops = d->isdmrg ? 2 : 3;
         int map[3] = {0, 1, 2}, inv[3] = {0, 1, 2};
         if (!d->isdmrg)
                 for (int j = 0; j < 3; ++j) { map[j] = d->map[j]; inv[map[j]] = j; }
-        memset(y, 0, sizeof *y * (size_t) d->block_off[d->nblocks]);
-
-        for (int nb = 0; nb < d->nblocks; ++nb) {
+        {
                 int dn[3];
                 for (int j = 0; j < 3; ++j) dn[j] = d->dims[3 * nb + map[j]];
                 if (d->isdmrg) dn[2] = 1;
@@ -122,6 +121,29 @@ int t3ns_oracle_matvec(const t3ns_heff_desc *d, const double *x, double *y)
                                 }
                         }
                 }
+        }
+}
+
+int t3ns_oracle_matvec(const t3ns_heff_desc *d, const double *x, double *y)
+{
+        memset(y, 0, sizeof *y * (size_t) d->block_off[d->nblocks]);
+        for (int nb = 0; nb < d->nblocks; ++nb) matvec_block(d, x, y, nb);
+        return 0;
+}
+
+/* The matvec restricted to the new blocks blocks[0..n): those blocks of y are
+ * computed exactly as t3ns_oracle_matvec computes them, every other element
+ * of y is left untouched.  Lets the tests check large steps on a sample of
+ * blocks in bounded CPU time. */
+int t3ns_oracle_matvec_blocks(const t3ns_heff_desc *d, const double *x, double *y,
+                              const int *blocks, int n)
+{
+        for (int i = 0; i < n; ++i) {
+                const int nb = blocks[i];
+                if (nb < 0 || nb >= d->nblocks) return -1;
+                const int64_t b0 = d->block_off[nb], b1 = d->block_off[nb + 1];
+                memset(y + b0, 0, sizeof *y * (size_t) (b1 - b0));
+                matvec_block(d, x, y, nb);
         }
         return 0;
 }

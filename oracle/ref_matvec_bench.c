@@ -158,12 +158,16 @@ int main(int argc, char **argv)
         hd.sr.shufid = malloc(sizeof *hd.sr.shufid * (size_t) nb);
         static const int ord3[6][3] = {{0,1,2},{1,0,2},{0,2,1},{1,2,0},{2,0,1},{2,1,0}};
         static const int ord2[2][2] = {{0,1},{1,0}};
-        double flops = 0;
+        double flops = 0, flops_full = 0;
         for (int i = 0; i < nb; ++i) {
                 for (int k = 0; k < 3; ++k) hd.sr.dimsofsb[i][k] = dims[3 * i + k];
-                hd.sr.nr_oldsb[i] = (i % stride == 0) ? pptr[i + 1] - pptr[i] : 0;
-                hd.sr.ntom[i] = malloc(sizeof **hd.sr.ntom * (size_t) (hd.sr.nr_oldsb[i] + 1));
-                for (int j = 0; j < hd.sr.nr_oldsb[i]; ++j) {
+                const int sampled = i % stride == 0;
+                const int npr = pptr[i + 1] - pptr[i];
+                hd.sr.nr_oldsb[i] = sampled ? npr : 0;
+                hd.sr.ntom[i] = malloc(sizeof **hd.sr.ntom * (size_t) (npr + 1));
+                /* every block's pairs are counted (flops_full); only the
+                 * sampled blocks keep them in the replay schedule */
+                for (int j = 0; j < npr; ++j) {
                         const int p = pptr[i] + j;
                         struct newtooldmatvec *t = &hd.sr.ntom[i][j];
                         t->oldsb = pold[p];
@@ -191,7 +195,10 @@ int main(int argc, char **argv)
                                                 const int sb = t->sbops[c][q];
                                                 ok = b[sb] != b[sb + 1];
                                         }
-                                        if (ok) flops += 2 * fl;
+                                        if (ok) {
+                                                flops_full += 2 * fl;
+                                                if (sampled) flops += 2 * fl;
+                                        }
                                 }
                         }
                 }
@@ -225,7 +232,9 @@ int main(int argc, char **argv)
         }
         qsort(ts, (size_t) calls, sizeof *ts, cmpd);
         printf("{\"seconds_per_matvec\": %.6e, \"calls\": %d, \"flops\": %.6e, "
+               "\"flops_full\": %.6e, \"sampled_blocks\": %d, \"blocks\": %d, "
                "\"rel_diff_vs_capture\": %.3e, \"size\": %d, \"stride\": %d}\n",
-               ts[calls / 2], calls, flops, sqrt(dn2 / (rn2 > 0 ? rn2 : 1)), size, stride);
+               ts[calls / 2], calls, flops, flops_full, (nb + stride - 1) / stride, nb,
+               sqrt(dn2 / (rn2 > 0 ? rn2 : 1)), size, stride);
         return 0;
 }

@@ -31,6 +31,7 @@
 
 #include "Heff.h"
 #include "bookkeeper.h"
+#include "davidson.h"
 #include "hamiltonian.h"
 #include "instructions.h"
 #include "macros.h"
@@ -611,8 +612,33 @@ static void usage(void)
         exit(2);
 }
 
+/* --precond-file IN OUT: one call of davidson_diagonal_preconditioner (the
+ * reference's in t3ns_run_ref, the drop-in's in t3ns_run_dropin) on the
+ * arrays of IN ({int64 n; double theta; double result[n], diagonal[n],
+ * vec_t[n]}); the resulting vec_t is written to OUT. */
+static int precond_file(const char *in, const char *out)
+{
+        FILE *f = fopen(in, "rb");
+        if (!f) return 2;
+        int64_t n = 0;
+        double theta = 0;
+        if (fread(&n, sizeof n, 1, f) != 1 || fread(&theta, sizeof theta, 1, f) != 1 || n <= 0 ||
+            n > INT32_MAX) { fclose(f); return 2; }
+        double *a = malloc(sizeof *a * 3 * (size_t) n);
+        if (!a || fread(a, sizeof *a, 3 * (size_t) n, f) != 3 * (size_t) n) { fclose(f); return 2; }
+        fclose(f);
+        davidson_diagonal_preconditioner(a, theta, (int) n, a + n, a + 2 * n);
+        f = fopen(out, "wb");
+        if (!f) return 2;
+        fwrite(a + 2 * n, sizeof *a, (size_t) n, f);
+        fclose(f);
+        free(a);
+        return 0;
+}
+
 int main(int argc, char **argv)
 {
+        if (argc == 4 && !strcmp(argv[1], "--precond-file")) return precond_file(argv[2], argv[3]);
         const char *net = NULL, *inter = NULL, *symm = "Z2,U1,SU2", *ts = NULL;
         char init = 'c';
         struct regime regs[16];

@@ -56,30 +56,49 @@ def build_engine(force: bool = False) -> str:
     return out
 
 
-REFERENCE_INCLUDE = os.environ.get("T3NS_REFERENCE_INCLUDE", "/root/reference/include")
 SHIM_INCLUDE = os.path.join(ROOT, "oracle", "shim")
 DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c", "bupdate_dropin.c", "dense_dropin.c"]
 
 
-def build_dropin(force: bool = False):
+def reference_checkout(reference: str | None = None) -> str:
+    """The reference T3NS checkout whose headers the drop-in is compiled
+    against: the argument, else $T3NS_REFERENCE.  Raises when neither names
+    a checkout."""
+    ref = reference or os.environ.get("T3NS_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, "include")):
+        raise RuntimeError("the reference checkout is not known: set T3NS_REFERENCE to the "
+                           "T3NS source tree (its include/ defines the drop-in's struct layouts)")
+    return ref
+
+
+def build_dropin(force: bool = False, reference: str | None = None):
     """libt3ns_dropin.so: the reference entry points on top of the engine.
     Compiled against the reference headers, whose struct layouts it must
-    match; skipped (returns None) when they are not available."""
-    if not os.path.isdir(REFERENCE_INCLUDE):
-        return None
+    match (reference_checkout())."""
+    ref_include = os.path.join(reference_checkout(reference), "include")
     engine = build_engine()
     out = os.path.join(LIBDIR, "libt3ns_dropin.so")
     srcs = [os.path.join(CSRC, "dropin", f) for f in DROPIN_SOURCES]
     if force or _stale(out, srcs + [engine, os.path.join(INCLUDE, "t3ns_b200.h")]):
         _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu11", "-w", "-DMAX_SYMMETRIES=5",
-              "-DNDEBUG", "-I", REFERENCE_INCLUDE, "-I", SHIM_INCLUDE, "-I", INCLUDE,
+              "-DNDEBUG", "-I", ref_include, "-I", SHIM_INCLUDE, "-I", INCLUDE,
               "-o", out, *srcs, "-L", LIBDIR, "-l:libt3ns_b200.so", "-Wl,-rpath,$ORIGIN",
               "-lpthread"])
     return out
 
 
-def build_all(force: bool = False):
-    return {"engine": build_engine(force), "dropin": build_dropin(force)}
+def build_all(force: bool = False, reference: str | None = None):
+    """The engine, and the drop-in when the reference checkout is known
+    (argument or $T3NS_REFERENCE); without it the drop-in is not rebuilt
+    and a message says so."""
+    out = {"engine": build_engine(force), "dropin": None}
+    try:
+        ref = reference_checkout(reference)
+    except RuntimeError as e:
+        print(f"drop-in not rebuilt: {e}", flush=True)
+        return out
+    out["dropin"] = build_dropin(force, ref)
+    return out
 
 
 if __name__ == "__main__":

@@ -139,12 +139,17 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
         return setup_precision(h, precision);
 }
 
-static int check_device_error(t3ns_heff *h)
+// Reads the kernel's error status after the work on stream s (the plan's
+// own stream when s is null): the copy is ordered after that work.
+static int check_device_error(t3ns_heff *h, cudaStream_t s = nullptr)
 {
+        if (!s) s = h->stream;
         int err = 0;
-        T3NS_CUDA_TRY(cudaMemcpy(&err, h->dp.err, sizeof(int), cudaMemcpyDeviceToHost));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(&err, h->dp.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        T3NS_CUDA_TRY(cudaStreamSynchronize(s));
         if (err) {
-                cudaMemset(h->dp.err, 0, sizeof(int));
+                T3NS_CUDA_TRY(cudaMemsetAsync(h->dp.err, 0, sizeof(int), s));
+                T3NS_CUDA_TRY(cudaStreamSynchronize(s));
                 return set_error(T3NS_E_DEVICE, "matvec kernel reported error status " +
                                                          std::to_string(err));
         }
@@ -191,6 +196,17 @@ int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y)
         T3NS_CUDA_TRY(cudaMemcpyAsync(y, h->stage_y, bytes, cudaMemcpyDeviceToHost, h->stream));
         T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
         return check_device_error(h);
+}
+
+int t3ns_heff_check_status(t3ns_heff *h, void *stream)
+{
+        if (!h) return set_error(T3NS_E_ARG, "null plan");
+        if (!stream) {
+                // legacy default stream: every blocking stream has drained
+                T3NS_CUDA_TRY(cudaStreamSynchronize(nullptr));
+                return check_device_error(h);
+        }
+        return check_device_error(h, (cudaStream_t) stream);
 }
 
 int t3ns_heff_diagonal_device(t3ns_heff *h, double *diag, void *stream)

@@ -457,10 +457,13 @@ using DevMatvec = std::function<int(const double *, double *, cudaStream_t)>;
 // kStallLevel * max(1, |energy|) -- the region where the split-precision
 // matvec's rounding (~2e-6 relative) can level it off -- and has not fallen
 // below 0.9 of its best value for `stall` iterations.
+// mv_err (optional): the matvec kernel's device error status; it is read back
+// with the iteration's scalars and a non-zero value ends the solve with
+// T3NS_E_DEVICE instead of continuing on a wrong product.
 static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, double *energy,
                          int max_vecs, int keep, double tol, int max_its, const double *d_diag,
                          t3ns_davidson_info *info, cudaStream_t s, int stall = 0,
-                         bool use_graphs = false)
+                         bool use_graphs = false, const int *mv_err = nullptr)
 {
         const auto t_start = std::chrono::steady_clock::now();
         if (max_vecs > kMaxVecs || keep > 4 || keep < 1 || keep >= max_vecs || max_vecs < 3)
@@ -536,6 +539,9 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                                               cudaMemcpyDeviceToHost, s));
                 T3NS_CUDA_TRY(cudaMemcpyAsync(b.host_scal + 4, b.status, sizeof(int),
                                               cudaMemcpyDeviceToHost, s));
+                if (mv_err)
+                        T3NS_CUDA_TRY(cudaMemcpyAsync(b.host_scal + 5, mv_err, sizeof(int),
+                                                      cudaMemcpyDeviceToHost, s));
                 precond_kernel<<<G, T, 0, s>>>(d_result, b.t, d_diag, b.scal, b.w, n);
                 T3NS_CUDA_TRY(cudaGetLastError());
                 return T3NS_OK;
@@ -586,6 +592,14 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                         return set_error(T3NS_E_CUDA, "davidson: iteration failed");
                 }
                 int st = 0;
+                if (mv_err) {
+                        memcpy(&st, b.host_scal + 5, sizeof(int));
+                        if (st != 0) {
+                                release();
+                                return set_error(T3NS_E_DEVICE, "davidson: matvec kernel reported "
+                                                                "error status " + std::to_string(st));
+                        }
+                }
                 memcpy(&st, b.host_scal + 4, sizeof(int));
                 if (st != 0) {
                         release();
@@ -635,16 +649,17 @@ int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
         const bool graphs = !ge || strcmp(ge, "0") != 0;
         if (h->precision == T3NS_PREC_FP64)
                 return davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy,
-                                     max_vecs, keep, tol, max_its, d_diag, info, s, 0, graphs);
+                                     max_vecs, keep, tol, max_its, d_diag, info, s, 0, graphs,
+                                     h->dp.err);
         // split-precision iterations, then FP64 defect correction from their vector
         t3ns_davidson_info i1{}, i2{};
         const auto t0 = std::chrono::steady_clock::now();
         int rc = davidson_core(h->hp.size, matvec_in(h->precision), d_result, energy, max_vecs,
-                               keep, tol, max_its, d_diag, &i1, s, /*stall=*/4, graphs);
+                               keep, tol, max_its, d_diag, &i1, s, /*stall=*/4, graphs, h->dp.err);
         if (rc < 0) return rc;
         rc = davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy, max_vecs,
                            keep, tol, std::max(max_its - i1.iterations, 2), d_diag, &i2, s, 0,
-                           graphs);
+                           graphs, h->dp.err);
         if (rc < 0) return rc;
         if (info) {
                 *info = i2;

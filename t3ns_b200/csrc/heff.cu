@@ -34,9 +34,11 @@
 //     reduction over the group inside each warp (single owner per output
 //     element: no atomics).
 #include <algorithm>
+#include <bitset>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -47,6 +49,7 @@
 namespace t3ns {
 
 constexpr int kGMax = 64;         // terms per group
+constexpr int kMaxDevices = 64;
 constexpr double kPairVisitCost = 4e4;   // FLOP-equivalent of one (unit, pair) visit
 
 // Kernel configurations.  The large one (one 512-thread CTA per SM, 208 KB of
@@ -951,6 +954,12 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                 if ((int64_t) e[0] * e[1] * e[2] != d->block_off[b + 1] - d->block_off[b])
                         return set_error(T3NS_E_ARG, "block size != product of dims at block " +
                                                           std::to_string(b));
+                // the kernels address elements inside one block (and inside one
+                // operator block, whose sizes are 32-bit in the descriptor) with
+                // 32-bit offsets; only the offsets of blocks are 64-bit
+                if ((int64_t) e[0] * e[1] * e[2] >= ((int64_t) 1 << 31))
+                        return set_error(T3NS_E_LIMIT, "block " + std::to_string(b) +
+                                                               " has 2^31 or more elements");
                 hp.edims[b] = make_int4(e[0], e[1], e[2], 0);
         }
         hp.size = d->block_off[d->nblocks];
@@ -1249,12 +1258,21 @@ template <class Cfg, class T>
 static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const T *x, const T *ops,
                       double *y, cudaStream_t s)
 {
-        static bool attr_set = false;   // per instantiation
-        if (!attr_set) {
-                T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_kernel<Cfg, T>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int) smem_bytes_t<Cfg, T>()));
-                attr_set = true;
+        // the shared-memory opt-in is a per-device attribute of the kernel:
+        // set once per device (per instantiation), under a lock
+        static std::mutex mu;
+        static std::bitset<kMaxDevices> attr_set;
+        int dev = 0;
+        T3NS_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) return set_error(T3NS_E_LIMIT, "device ordinal too large");
+        {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!attr_set[dev]) {
+                        T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_kernel<Cfg, T>,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           (int) smem_bytes_t<Cfg, T>()));
+                        attr_set[dev] = true;
+                }
         }
         const int share = dp.share ? std::max(1, dp.share->load(std::memory_order_relaxed)) : 1;
         const int grid = std::max(1, dt.grid / share);

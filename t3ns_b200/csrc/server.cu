@@ -104,7 +104,12 @@ struct t3ns_server {
                 t3ns_heff *h = nullptr;
                 double *d_res = nullptr, *d_diag = nullptr;
                 int rc = t3ns_heff_create(r->desc, r->precision, &h);
-                if (rc == T3NS_OK) rc = t3ns_heff_autotune(h, 1, 0, nullptr);
+                // tune only while this solve has the GPU to itself: timings taken
+                // beside other solves are skewed and would be cached for the size
+                // bucket (later plans, here and elsewhere, start on the cached
+                // choice); otherwise the plan keeps the bucket's cached or default
+                // configuration
+                if (rc == T3NS_OK && running.load() <= 1) rc = t3ns_heff_autotune(h, 1, 0, nullptr);
                 if (rc == T3NS_OK) h->dp.share = &running;
                 const int64_t n = r->desc->block_off[r->desc->nblocks];
                 const size_t bytes = sizeof(double) * (size_t) std::max<int64_t>(n, 1);

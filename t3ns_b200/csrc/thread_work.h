@@ -50,6 +50,10 @@ struct ThreadWork {
                         st = nullptr;
                         return set_error(T3NS_E_CUDA, "workspace: stream creation failed");
                 }
+                // a previous call that returned early on an error may have left
+                // copies in flight that still read or write the buffers: drain
+                // the stream before the caller touches them again
+                T3NS_CUDA_TRY(cudaStreamSynchronize(st));
                 if (dbytes > dev_bytes) {
                         T3NS_CUDA_TRY(cudaStreamSynchronize(st));
                         const size_t want = std::max(dbytes, 2 * dev_bytes);

@@ -116,3 +116,32 @@ def test_reference_energy_pin_n2(net, symm, ts):
                            "--regime", "1000,1000,1e-4,2,1e-6,4,2,1e-8,0",
                            "--regime", "1000,1000,1e-4,2,1e-6,100,10,1e-8,0", "--init", "c"])
     assert abs(energy(out) + 107.648250974014) < 1e-8
+
+
+@pytest.mark.gpu
+def test_dropin_preconditioner_matches_restated_reference(tmp_path):
+    """The drop-in's davidson_diagonal_preconditioner (the unchanged driver's
+    symbol, linked into t3ns_run_dropin) against the numpy restatement of
+    reference src/davidson.c:223-257 (oracle/precond_oracle.py, itself pinned
+    to the reference build on the CPU), cutoff branch included."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import precond_oracle
+    need(RUN_DROPIN)
+    rng = np.random.default_rng(11)
+    n, theta = 200_003, 0.35
+    r = rng.standard_normal(n)
+    r /= np.linalg.norm(r)
+    dg = rng.uniform(-3.0, 5.0, n)
+    dg[::977] = theta
+    t = rng.standard_normal(n) * 1e-3
+    fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
+    with open(fin, "wb") as f:
+        f.write(np.array([n], np.int64).tobytes())
+        f.write(np.array([theta]).tobytes())
+        for a in (r, dg, t):
+            f.write(a.tobytes())
+    subprocess.run([RUN_DROPIN, "--precond-file", str(fin), str(fout)], check=True, timeout=300)
+    got = np.fromfile(fout, np.float64)
+    want = precond_oracle.precondition(r, theta, dg, t)
+    assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)

@@ -29,3 +29,59 @@ def test_oracle_detects_planted_error():
     s["sr.combo_pref"][::7] *= 1.0 + 1e-9
     y = oracle_lib.matvec(StepDesc(s), s["x0"])
     assert np.linalg.norm(y - s["y0"]) > 1e-14 * np.linalg.norm(s["y0"])
+
+
+@pytest.mark.parametrize("path", golden_steps(), ids=lambda p: p.split("/")[-1])
+def test_block_sampled_oracle_equals_full_oracle(path):
+    """The block-restricted oracle (used on steps too large for the full one)
+    gives exactly the full oracle's values on the blocks it computes."""
+    s = read_step(path)
+    d = StepDesc(s)
+    full = oracle_lib.matvec(d, s["x0"])
+    blocks = oracle_lib.sample_blocks(s, k=6)
+    part = oracle_lib.matvec_blocks(d, s["x0"], blocks)
+    off = s["beginblock"].astype(np.int64)
+    for b in blocks:
+        assert np.array_equal(part[off[b]:off[b + 1]], full[off[b]:off[b + 1]])
+
+
+def _ref_lib():
+    import ctypes as C
+    import os
+
+    from conftest import ROOT
+    p = os.path.join(ROOT, "oracle", "_ref", "libt3ns_ref.so")
+    if not os.path.exists(p):
+        pytest.skip("reference library not built (make -C oracle)")
+    return C.CDLL(p, mode=C.RTLD_GLOBAL)
+
+
+@pytest.mark.parametrize("theta", [0.7, -1.25])
+def test_preconditioner_oracle_matches_reference(theta):
+    """oracle/precond_oracle.py against the reference's own
+    davidson_diagonal_preconditioner (src/davidson.c:223-257) from the
+    reference build, including diagonal entries exactly at theta (the
+    1e-12 cutoff branch)."""
+    import ctypes as C
+    import os
+    import sys
+
+    from conftest import ROOT
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import precond_oracle
+    f = _ref_lib().davidson_diagonal_preconditioner
+    f.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+    f.restype = None
+    rng = np.random.default_rng(5)
+    n = 50_001
+    r = rng.standard_normal(n)
+    r /= np.linalg.norm(r)
+    dg = rng.uniform(-3.0, 5.0, n)
+    dg[::977] = theta
+    dg[1::1013] = theta + 5e-13          # inside the cutoff, positive side
+    dg[2::1019] = theta - 5e-13          # inside the cutoff, negative side
+    t = rng.standard_normal(n) * 1e-3
+    out = t.copy()
+    f(r.ctypes.data, theta, n, dg.ctypes.data, out.ctypes.data)
+    want = precond_oracle.precondition(r, theta, dg, t)
+    assert np.linalg.norm(out - want) <= 1e-14 * np.linalg.norm(want)

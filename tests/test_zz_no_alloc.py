@@ -6,17 +6,26 @@ synchronisation of cudaMalloc/cudaFree) call
 t3ns_precondition_device_noalloc with their own device buffers; its only
 scratch is a fixed array inside the library.  This test calls it through the
 C ABI twice in a row, on different inputs, and checks each result against
-the allocating entry point t3ns_precondition_host within the 1e-12 relative
-tolerance of the other parity tests; it also checks the size limit is
-enforced.  It lives in its own file, collected last, and passes alone in a
+the allocating entry point t3ns_precondition_host and against the CPU
+restatement of the reference's preconditioner (oracle/precond_oracle.py,
+reference src/davidson.c:223-257, cutoff branch included), within the
+1e-12 relative tolerance of the other parity tests; the second, smaller call
+also shows that nothing of the first call's scratch leaks into it.  It also
+checks the size limit is enforced.  It lives in its own file, collected last, and passes alone in a
 fresh process as well as after the other tests.
 """
 import ctypes as C
+import os
+import sys
 
 import numpy as np
 import pytest
 
+from conftest import ROOT
 from t3ns_b200 import native
+
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import precond_oracle  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -69,6 +78,9 @@ def test_noalloc_matches_allocating_entry_point(torch_cuda):
         native.check(rc, "precondition_device_noalloc")
         got = d_t.cpu().numpy()
         err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert err <= RTOL, (call, err)
+        want = precond_oracle.precondition(result, theta, diag, vec_t)
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert err <= RTOL, (call, err)
 
 
