@@ -125,9 +125,11 @@ int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag);
 /* Kernel configurations of the matvec: 0 = one 512-thread CTA per SM with
  * large shared-memory output tiles, 1 = two 256-thread CTAs per SM with small
  * tiles, 2 = one 768-thread CTA per SM (more warps, fewer registers a thread)
- * with mid-size tiles.  Each has its own tiling of the plan (built on first
- * use). */
-#define T3NS_NUM_CONFIGS 3
+ * with mid-size tiles; 3 and 4 = the contraction-ordered kernel (every stage
+ * contracts the fastest axis of its input, operators transposed on the
+ * device) with 768 and 512 threads, FP64 only.  Each has its own tiling of the
+ * plan (built on first use). */
+#define T3NS_NUM_CONFIGS 5
 int t3ns_heff_set_config(t3ns_heff *h, int config);
 int t3ns_heff_get_config(const t3ns_heff *h);
 

@@ -59,9 +59,50 @@ static std::tuple<int, int, int, int> size_bucket(const HostPlan &hp, int precis
         return {lg((double) hp.size), lg((double) maxblk), lg(hp.flops_ref), precision};
 }
 
+// Transposed operators of the contraction-ordered configurations (built on
+// the device from the resident operators, on first use).
+static int setup_transposed(t3ns_heff *h)
+{
+        DevicePlan &dp = h->dp;
+        if (dp.ops_t) return T3NS_OK;
+        const HostPlan &hp = h->hp;
+        T3NS_TRY(upload(h, &dp.toff, hp.toff.data(), hp.toff.size()));
+        T3NS_TRY(dev_alloc(h, &dp.ops_t, (size_t) hp.opt_elems));
+        int64_t *d_jobs = nullptr;
+        if (!hp.tjobs.empty()) {
+                T3NS_CUDA_TRY(cudaMalloc(&d_jobs, sizeof(int64_t) * hp.tjobs.size()));
+                const cudaError_t e = cudaMemcpy(d_jobs, hp.tjobs.data(), sizeof(int64_t) * hp.tjobs.size(),
+                                                 cudaMemcpyHostToDevice);
+                int rc = e == cudaSuccess ? build_transposed_ops(hp, dp, d_jobs, h->stream)
+                                          : set_error(T3NS_E_CUDA, "transposed operators: upload");
+                if (rc == T3NS_OK && cudaStreamSynchronize(h->stream) != cudaSuccess)
+                        rc = set_error(T3NS_E_CUDA, "transposed operators: kernel");
+                cudaFree(d_jobs);
+                T3NS_TRY(rc);
+        }
+        return T3NS_OK;
+}
+
+// {hi, lo} pairs of the transposed operators (split precision on the
+// contraction-ordered configurations).
+static int setup_transposed_split(t3ns_heff *h)
+{
+        DevicePlan &dp = h->dp;
+        if (dp.ops_t_split) return T3NS_OK;
+        T3NS_TRY(setup_transposed(h));
+        T3NS_TRY(dev_alloc(h, &dp.ops_t_split, (size_t) h->hp.opt_elems));
+        T3NS_TRY(convert_to_pairs(dp.ops_t, dp.ops_t_split, h->hp.opt_elems, h->stream));
+        T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return T3NS_OK;
+}
+
 // Device copy of the tiling for configuration cfg (tiled on first use).
 static int upload_tiles(t3ns_heff *h, int cfg)
 {
+        if (kCfgs[cfg].v2) {
+                T3NS_TRY(setup_transposed(h));
+                if (h->precision == T3NS_PREC_3XTF32) T3NS_TRY(setup_transposed_split(h));
+        }
         DeviceTiles &dt = h->dp.tiles[cfg];
         if (dt.built) return T3NS_OK;
         T3NS_TRY(tile_plan(h->hp, cfg));
@@ -94,6 +135,7 @@ static int setup_precision(t3ns_heff *h, int precision)
                 T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
         }
         h->precision = precision;
+        if (precision == T3NS_PREC_3XTF32 && dp.ops_t) T3NS_TRY(setup_transposed_split(h));
         return T3NS_OK;
 }
 
@@ -260,6 +302,7 @@ int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
         int best = h->dp.active;
         double best_ms = 0;
         int rc = T3NS_OK;
+        bool first = true;
         for (int c = 0; c < kNumCfgs && rc == T3NS_OK; ++c) {
                 rc = t3ns_heff_set_config(h, c);
                 if (rc != T3NS_OK) break;
@@ -281,9 +324,10 @@ int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
                 std::sort(t.begin(), t.end());
                 const double med = t[t.size() / 2];
                 if (ms_out) ms_out[c] = med;
-                if (c == 0 || med < best_ms) {
+                if (first || med < best_ms) {
                         best = c;
                         best_ms = med;
+                        first = false;
                 }
         }
         cudaEventDestroy(e0);

@@ -41,10 +41,13 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "common.h"
 #include "heff_internal.h"
+#include "heff_v2.cuh"
 
 namespace t3ns {
 
@@ -70,13 +73,28 @@ struct CfgWide {
         static constexpr int kThreads = 768, kMinBlocks = 1;
         static constexpr int kOut = 6144, kPsi = 1024, kW = 19456;
 };
+// Contraction-ordered kernel (heff_v2.cuh): 768 threads with 6,144-element
+// output tiles, and 512 threads with 8,192; both stage old blocks of up to
+// 4,096 padded elements.
+struct CfgV2Wide {
+        static constexpr int kThreads = 768, kMinBlocks = 1;
+        static constexpr int kOut = 6144, kPsi = 4096, kW = 17408;
+};
+struct CfgV2Large {
+        static constexpr int kThreads = 512, kMinBlocks = 1;
+        static constexpr int kOut = 8192, kPsi = 4096, kW = 15360;
+};
 const KernelCfg kCfgs[kNumCfgs] = {
         {CfgLarge::kThreads, CfgLarge::kMinBlocks, CfgLarge::kOut, CfgLarge::kPsi, CfgLarge::kW,
-         "fp64-512x1-out8192"},
+         "fp64-512x1-out8192", 0},
         {CfgSmall::kThreads, CfgSmall::kMinBlocks, CfgSmall::kOut, CfgSmall::kPsi, CfgSmall::kW,
-         "fp64-256x2-out3072"},
+         "fp64-256x2-out3072", 0},
         {CfgWide::kThreads, CfgWide::kMinBlocks, CfgWide::kOut, CfgWide::kPsi, CfgWide::kW,
-         "fp64-768x1-out6144"},
+         "fp64-768x1-out6144", 0},
+        {CfgV2Wide::kThreads, CfgV2Wide::kMinBlocks, CfgV2Wide::kOut, CfgV2Wide::kPsi, CfgV2Wide::kW,
+         "fp64-ordered-768x1-out6144", 1},
+        {CfgV2Large::kThreads, CfgV2Large::kMinBlocks, CfgV2Large::kOut, CfgV2Large::kPsi,
+         CfgV2Large::kW, "fp64-ordered-512x1-out8192", 1},
 };
 
 
@@ -136,7 +154,17 @@ struct RowSplit {
 // advanced in place (no per-element index arithmetic or K bound) and a
 // predicated tail step.  Loop bounds are warp-uniform (mma.sync needs the
 // whole warp); lanes outside M or N read row / column 0 and use zeros.
-template <int RM, int RN>
+// Loads of one operand: the operator side (A_OP: A is the operator) reads
+// global memory through the read-only path, the other side is the staged
+// block or an intermediate in shared memory.
+template <bool GLOBAL_RO>
+__device__ __forceinline__ double ld_opnd(const double *p)
+{
+        if constexpr (GLOBAL_RO) return __ldg(p);
+        else return *p;
+}
+
+template <int RM, int RN, bool A_OP>
 __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const double *Ab, int ak,
                                               const RowSplit &rs, const double *Bb, int bk,
                                               int bn, int K, int M, int N, int m0, int n0, int lr,
@@ -162,12 +190,12 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
         auto load_step = [&]() {
 #pragma unroll
                 for (int i = 0; i < RM; ++i) {
-                        a[i] = mok[i] ? *ap[i] : 0.0;
+                        a[i] = mok[i] ? ld_opnd<A_OP>(ap[i]) : 0.0;
                         ap[i] += astep;
                 }
 #pragma unroll
                 for (int j = 0; j < RN; ++j) {
-                        b[j] = nok[j] ? *bp[j] : 0.0;
+                        b[j] = nok[j] ? ld_opnd<!A_OP>(bp[j]) : 0.0;
                         bp[j] += bstep;
                 }
         };
@@ -190,9 +218,9 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
         if (K & 3) {
                 const bool kok = lc < (K & 3);
 #pragma unroll
-                for (int i = 0; i < RM; ++i) a[i] = (mok[i] && kok) ? *ap[i] : 0.0;
+                for (int i = 0; i < RM; ++i) a[i] = (mok[i] && kok) ? ld_opnd<A_OP>(ap[i]) : 0.0;
 #pragma unroll
-                for (int j = 0; j < RN; ++j) b[j] = (nok[j] && kok) ? *bp[j] : 0.0;
+                for (int j = 0; j < RN; ++j) b[j] = (nok[j] && kok) ? ld_opnd<!A_OP>(bp[j]) : 0.0;
 #pragma unroll
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -205,8 +233,8 @@ __device__ __forceinline__ void warp_tile_mma(double (&d)[RM][RN][2], const doub
 // loop runs ceil(K/4) steps (the last predicated when K % 4 != 0) and the
 // final step of a term already loads the first step of the next term, so a
 // term's start does not wait on its operand loads.
-template <int RM, int RN>
-__device__ __forceinline__ void warp_tile_mma_terms(double (&d)[RM][RN][2], int ax,
+template <int RM, int RN, int AX>
+__device__ __forceinline__ void warp_tile_mma_terms(double (&d)[RM][RN][2],
                                                     const double *__restrict__ ops,
                                                     const int64_t *opoff, const double *in,
                                                     int in_gs, int g0, int g1, int gstep, int ak,
@@ -234,7 +262,7 @@ __device__ __forceinline__ void warp_tile_mma_terms(double (&d)[RM][RN][2], int 
         auto set_term = [&](int g) {
                 const double *op = ops + opoff[g];
                 const double *tin = in + (int64_t) g * in_gs;
-                const double *Ab = ax == 0 ? op : tin, *Bb = ax == 0 ? tin : op;
+                const double *Ab = AX == 0 ? op : tin, *Bb = AX == 0 ? tin : op;
 #pragma unroll
                 for (int i = 0; i < RM; ++i) ap[i] = Ab + ao[i];
 #pragma unroll
@@ -245,12 +273,12 @@ __device__ __forceinline__ void warp_tile_mma_terms(double (&d)[RM][RN][2], int 
                 const bool kok = st + 1 < S || rem == 0 || lc < rem;
 #pragma unroll
                 for (int i = 0; i < RM; ++i) {
-                        a[i] = (mok[i] && kok) ? *ap[i] : 0.0;
+                        a[i] = (mok[i] && kok) ? ld_opnd<AX == 0>(ap[i]) : 0.0;
                         ap[i] += astep;
                 }
 #pragma unroll
                 for (int j = 0; j < RN; ++j) {
-                        b[j] = (nok[j] && kok) ? *bp[j] : 0.0;
+                        b[j] = (nok[j] && kok) ? ld_opnd<AX != 0>(bp[j]) : 0.0;
                         bp[j] += bstep;
                 }
         };
@@ -285,8 +313,8 @@ __device__ __forceinline__ void warp_tile_mma_terms(double (&d)[RM][RN][2], int 
 // `out` instead (which then has no term stride).  Each warp owns
 // (8*RM) x (8*RN) output tiles and runs their K loop on the FP64 tensor
 // pipe; with ACC the group reduction stays inside the warp's accumulators.
-template <bool ACC, int RM, int RN, int NW>
-__device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, int ldop, int G,
+template <bool ACC, int RM, int RN, int NW, int AX>
+__device__ __forceinline__ void grouped_stage_t(const int *w, int rows, int ldop, int G,
                                                 const int64_t *opoff,
                                                 const double *__restrict__ ops, const double *in,
                                                 int in_gs, double *out, int out_gs,
@@ -297,10 +325,10 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
         RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
         // A(m,k) = Ab[rs.a_off(m) + k*ak], B(k,n) = Bb[k*bk + n*bn],
         // C(m,n) = Cb[rs.c_off(m) + n*cn]
-        if (ax == 0) {
+        if constexpr (AX == 0) {
                 M = rows; N = w[1] * w[2]; K = w[0];
                 ak = ldop; bk = 1; bn = K; cn = rows;
-        } else if (ax == 1) {
+        } else if constexpr (AX == 1) {
                 M = w[0] * w[2]; N = rows; K = w[1];
                 ak = w[0]; bk = ldop; bn = 1; cn = w[0];
                 rs = RowSplit{w[0], 1.0f / w[0], (int64_t) w[0] * w[1], (int64_t) w[0] * rows};
@@ -339,15 +367,18 @@ __device__ __forceinline__ void grouped_stage_t(int ax, const int *w, int rows, 
                 for (int i = 0; i < RM; ++i)
 #pragma unroll
                         for (int j = 0; j < RN; ++j) d[i][j][0] = d[i][j][1] = 0.0;
-                if (ACC) {
-                        warp_tile_mma_terms<RM, RN>(d, ax, ops, opoff, in, in_gs, g0, g1, gstep, ak,
-                                                    rs, bk, bn, K, M, N, m0, n0, lr, lc);
+                if constexpr (ACC) {
+                        warp_tile_mma_terms<RM, RN, AX>(d, ops, opoff, in, in_gs, g0, g1, gstep, ak,
+                                                        rs, bk, bn, K, M, N, m0, n0, lr, lc);
                 } else {
                         const double *op = ops + opoff[g0];
                         const double *tin = in + g0 * in_gs;
-                        const double *Ab = ax == 0 ? op : tin;
-                        const double *Bb = ax == 0 ? tin : op;
-                        warp_tile_mma<RM, RN>(d, Ab, ak, rs, Bb, bk, bn, K, M, N, m0, n0, lr, lc);
+                        if constexpr (AX == 0)
+                                warp_tile_mma<RM, RN, true>(d, op, ak, rs, tin, bk, bn, K, M, N, m0,
+                                                            n0, lr, lc);
+                        else
+                                warp_tile_mma<RM, RN, false>(d, tin, ak, rs, op, bk, bn, K, M, N, m0,
+                                                             n0, lr, lc);
                 }
                 const double sc = (!ACC && scale) ? scale[g0] : 1.0;
                 double *Cb = out + (ACC ? 0 : g0 * out_gs);
@@ -397,15 +428,23 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
 {
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
-        if (M <= 8)
-                grouped_stage_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
-                                               scratch, scratch_cap);
-        else if (N <= 8)
-                grouped_stage_t<ACC, 4, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
-                                               scratch, scratch_cap);
-        else
-                grouped_stage_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
-                                               scratch, scratch_cap);
+        // the stage axis is a template parameter: it fixes which operand is
+        // the operator (global) and which the staged data (shared memory)
+        auto go = [&](auto axc) {
+                constexpr int AX = decltype(axc)::value;
+                if (M <= 8)
+                        grouped_stage_t<ACC, 1, 4, NW, AX>(w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                           out_gs, scale, scratch, scratch_cap);
+                else if (N <= 8)
+                        grouped_stage_t<ACC, 4, 1, NW, AX>(w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                           out_gs, scale, scratch, scratch_cap);
+                else
+                        grouped_stage_t<ACC, 2, 2, NW, AX>(w, rows, ldop, G, opoff, ops, in, in_gs, out,
+                                                           out_gs, scale, scratch, scratch_cap);
+        };
+        if (ax == 0) go(std::integral_constant<int, 0>{});
+        else if (ax == 1) go(std::integral_constant<int, 1>{});
+        else go(std::integral_constant<int, 2>{});
 }
 
 // ---------------------------------------------------------------------------
@@ -761,9 +800,16 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                                         PREF[tid] = (Scale) tk.pref;
                                 }
                                 __syncthreads();
+                                // the first stage reads the staged block (shared memory) or
+                                // the block in global memory: one call site for each, so each
+                                // is compiled for its own address space
                                 if (nst == 3) {
-                                        grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
-                                                             ops, in0, 0, W1, s1, nullptr);
+                                        if (in0 == PSI)
+                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
+                                                                     OPOFF, ops, PSI, 0, W1, s1, nullptr);
+                                        else
+                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
+                                                                     OPOFF, ops, xin, 0, W1, s1, nullptr);
                                         __syncthreads();
                                         grouped_stage<false, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
                                                              OPOFF + kGMax, ops, W1, s1, W2, s2, PREF);
@@ -773,8 +819,12 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                                                             OPOFF + 2 * kGMax, ops, W2, s2, OUT, 0,
                                                             nullptr, W1, G * s1);
                                 } else {
-                                        grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g, OPOFF,
-                                                             ops, in0, 0, W1, s1, PREF);
+                                        if (in0 == PSI)
+                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
+                                                                     OPOFF, ops, PSI, 0, W1, s1, PREF);
+                                        else
+                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
+                                                                     OPOFF, ops, xin, 0, W1, s1, PREF);
                                         __syncthreads();
                                         grouped_stage<true, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
                                                             OPOFF + kGMax, ops, W1, s1, OUT, 0,
@@ -797,6 +847,217 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                 }
                 __syncthreads();
         }
+}
+
+template <class Cfg>
+constexpr size_t smem_bytes_v2()
+{
+        return sizeof(double) * (Cfg::kOut + Cfg::kPsi + Cfg::kW + kGMax) +
+               sizeof(int64_t) * 3 * kGMax + 3 * sizeof(v2::Geo) + 64;
+}
+
+// The matvec with contraction-ordered layouts (heff_v2.cuh): persistent CTAs
+// take units off the counter as heff_kernel does; per pair the old block is
+// staged permuted for the pair's sequence, and the stages run on the
+// transposed operators ops_t (offsets toff per task and memory axis).  SPLIT:
+// 3xTF32 products of {hi, lo} pairs (ops_t holds pairs, the staged block and
+// the intermediates too), FP64 output tile.
+template <class Cfg, bool SPLIT>
+__global__ void __launch_bounds__(Cfg::kThreads, Cfg::kMinBlocks)
+heff_v2_kernel(const double *__restrict__ x, double *__restrict__ y,
+               const typename std::conditional<SPLIT, float2, double>::type *__restrict__ ops_t,
+               const int64_t *__restrict__ blk_off, const int4 *__restrict__ edims,
+               const HeffUnit *__restrict__ units, int n_units, const HeffPair *__restrict__ pairs,
+               const HeffTask *__restrict__ tasks, const int64_t *__restrict__ toff, int *counter,
+               int *err)
+{
+        using E = typename std::conditional<SPLIT, float2, double>::type;
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        constexpr int kThreads = Cfg::kThreads, NW = Cfg::kThreads / 32;
+        double *OUT = reinterpret_cast<double *>(smem_raw);
+        E *PSI = reinterpret_cast<E *>(OUT + Cfg::kOut);
+        E *W = PSI + Cfg::kPsi;
+        double *PREF = reinterpret_cast<double *>(W + Cfg::kW);
+        int64_t *OPOFF = reinterpret_cast<int64_t *>(PREF + kGMax);   // [3][kGMax]
+        v2::Geo *GEO = reinterpret_cast<v2::Geo *>(OPOFF + 3 * kGMax);   // [3]
+        int *UNIT = reinterpret_cast<int *>(GEO + 3);
+        const int tid = threadIdx.x;
+
+        for (;;) {
+                if (tid == 0) *UNIT = atomicAdd(counter, 1);
+                __syncthreads();
+                const int u = *UNIT;
+                __syncthreads();
+                if (u >= n_units) break;
+                const HeffUnit un = units[u];
+                const int nb = un.nb;
+                const int4 en = edims[nb];
+                const int dn[3] = {en.x, en.y, en.z};
+                const int ext[3] = {un.at, un.bt, un.ct};
+                const int row0[3] = {un.a0, un.b0, un.c0};
+                const int st = ext[0] * ext[1] * ext[2];
+                for (int e = tid; e < st; e += kThreads) OUT[e] = 0.0;
+                __syncthreads();
+                for (int p = un.p0; p < un.p1; ++p) {
+                        const HeffPair pr = pairs[p];
+                        const int4 eo = edims[pr.old];
+                        const int o[3] = {eo.x, eo.y, eo.z};
+                        const int nst = (pr.axes >> 6) & 3;
+                        int seq[3];
+                        seq[0] = pr.axes & 3;
+                        seq[1] = (pr.axes >> 2) & 3;
+                        seq[2] = nst == 3 ? (pr.axes >> 4) & 3 : 3 - seq[0] - seq[1];
+                        const int psz = v2::staged_ld(o[seq[0]]) * o[seq[1]] * o[seq[2]];
+                        const bool staged = psz <= Cfg::kPsi;
+                        if (!staged && seq[0] != 0) {
+                                // the plan starts every sequence of an unstaged block on axis 0
+                                if (tid == 0) atomicExch(err, 4);
+                                return;
+                        }
+                        if (tid == 0) {
+                                const int ostr[3] = {1, ext[0], ext[0] * ext[1]};
+                                v2::make_geos(GEO, nst, seq, o, ext, staged, ostr);
+                        }
+                        __syncthreads();
+                        const int s1 = GEO[0].out_size, s2 = nst == 3 ? GEO[1].out_size : 0;
+                        if (s1 + s2 > Cfg::kW) {
+                                if (tid == 0) atomicExch(err, 3);
+                                return;
+                        }
+                        const double *xin = x + blk_off[pr.old];
+                        if (staged) {
+                                // old block -> (s0 padded, s1, s2), padding zeroed
+                                const int ld = v2::staged_ld(o[seq[0]]);
+                                const int K = o[seq[0]], d1 = o[seq[1]];
+                                const int str[3] = {1, o[0], o[0] * o[1]};
+                                const int sk = str[seq[0]], s1s = str[seq[1]], s2s = str[seq[2]];
+                                const float rld = 1.0f / ld, rd1 = 1.0f / d1;
+                                for (int e = tid; e < psz; e += kThreads) {
+                                        int k;
+                                        const int col = v2::divmod(e, ld, rld, k);
+                                        double v = 0.0;
+                                        if (k < K) {
+                                                int i1;
+                                                const int i2 = v2::divmod(col, d1, rd1, i1);
+                                                v = xin[k * sk + i1 * s1s + i2 * s2s];
+                                        }
+                                        if constexpr (SPLIT) PSI[e] = v2::split_pair(v);
+                                        else PSI[e] = v;
+                                }
+                        }
+                        const int G = min(kGMax, Cfg::kW / (s1 + s2));
+                        E *W1 = W, *W2 = W + G * s1;
+                        const int nterm = pr.t1 - pr.t0;
+                        for (int t0 = 0; t0 < nterm; t0 += G) {
+                                const int gg = min(G, nterm - t0);
+                                if (tid < gg) {
+                                        const int t = pr.t0 + t0 + tid;
+                                        for (int j = 0; j < nst; ++j)
+                                                OPOFF[j * kGMax + tid] = toff[3 * (int64_t) t + seq[j]] +
+                                                                         (int64_t) row0[seq[j]] * GEO[j].lda;
+                                        PREF[tid] = tasks[t].pref;
+                                }
+                                __syncthreads();
+                                const double *sc0 = nst == 3 ? nullptr : PREF;
+                                if constexpr (SPLIT) {
+                                        float *scr3 = reinterpret_cast<float *>(W1);
+                                        float *scr2 = reinterpret_cast<float *>(W1 + G * s1);
+                                        if (staged)
+                                                v2::stage_x<false, NW, false>(GEO[0], gg, OPOFF, ops_t, PSI, 0, W1,
+                                                                              s1, sc0);
+                                        else
+                                                v2::stage_x<false, NW, true>(GEO[0], gg, OPOFF, ops_t, xin, 0, W1,
+                                                                             s1, sc0);
+                                        __syncthreads();
+                                        if (nst == 3) {
+                                                v2::stage_x<false, NW, false>(GEO[1], gg, OPOFF + kGMax, ops_t, W1,
+                                                                              s1, W2, s2, PREF);
+                                                __syncthreads();
+                                                v2::stage_x<true, NW, false>(GEO[2], gg, OPOFF + 2 * kGMax, ops_t,
+                                                                             W2, s2, OUT, 0, nullptr, scr3,
+                                                                             2 * G * s1);
+                                        } else {
+                                                v2::stage_x<true, NW, false>(GEO[1], gg, OPOFF + kGMax, ops_t, W1,
+                                                                             s1, OUT, 0, nullptr, scr2,
+                                                                             2 * (Cfg::kW - G * s1));
+                                        }
+                                } else {
+                                        // the first stage reads the staged block (shared memory) or
+                                        // the block in place (global memory): one call site for each
+                                        if (staged)
+                                                v2::stage<false, NW, false>(GEO[0], gg, OPOFF, ops_t, PSI, 0, W1, s1,
+                                                                            sc0);
+                                        else
+                                                v2::stage<false, NW, true>(GEO[0], gg, OPOFF, ops_t, xin, 0, W1, s1,
+                                                                           sc0);
+                                        __syncthreads();
+                                        if (nst == 3) {
+                                                v2::stage<false, NW, false>(GEO[1], gg, OPOFF + kGMax, ops_t, W1, s1,
+                                                                            W2, s2, PREF);
+                                                __syncthreads();
+                                                // the last stage reads W2 only: W1's share is its scratch
+                                                v2::stage<true, NW, false>(GEO[2], gg, OPOFF + 2 * kGMax, ops_t, W2,
+                                                                           s2, OUT, 0, nullptr, W1, G * s1);
+                                        } else {
+                                                v2::stage<true, NW, false>(GEO[1], gg, OPOFF + kGMax, ops_t, W1, s1,
+                                                                           OUT, 0, nullptr, W1 + G * s1,
+                                                                           Cfg::kW - G * s1);
+                                        }
+                                }
+                                __syncthreads();
+                        }
+                }
+                double *yn = y + blk_off[nb];
+                for (int e = tid; e < st; e += kThreads) {
+                        const int a = e % ext[0];
+                        const int t = e / ext[0];
+                        const int b = t % ext[1];
+                        const int c = t / ext[1];
+                        double *dst = yn + (row0[0] + a) +
+                                      (int64_t) dn[0] * ((row0[1] + b) + (int64_t) dn[1] * (row0[2] + c));
+                        if (un.split) atomicAdd(dst, OUT[e]);
+                        else *dst = OUT[e];
+                }
+                __syncthreads();
+        }
+}
+
+// {hi, lo} pairs of the transposed operators (split-precision matvec of the
+// contraction-ordered configurations).
+__global__ void split_pairs_kernel(const double *__restrict__ a, float2 *__restrict__ b, int64_t n)
+{
+        for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+             i += (int64_t) gridDim.x * blockDim.x)
+                b[i] = v2::split_pair(a[i]);
+}
+
+// Transposes the referenced operator blocks into the layout of the
+// contraction-ordered kernel: job j = {src, dst, rows, cols} of a (rows x
+// cols) column-major block at ops[src] -> row-major at opt[dst] with rows of
+// v2::op_ld(cols) doubles (the padding zeroed).
+__global__ void transpose_ops_kernel(const double *__restrict__ ops, double *__restrict__ opt,
+                                     const int64_t *__restrict__ jobs, int64_t njobs)
+{
+        for (int64_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+                const int64_t src = jobs[4 * j], dst = jobs[4 * j + 1];
+                const int rows = (int) jobs[4 * j + 2], cols = (int) jobs[4 * j + 3];
+                const int ld = v2::op_ld(cols);
+                const int n = rows * ld;
+                for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                        const int r = e / ld, k = e - r * ld;
+                        opt[dst + e] = k < cols ? ops[src + r + (int64_t) k * rows] : 0.0;
+                }
+        }
+}
+
+int build_transposed_ops(const HostPlan &hp, DevicePlan &dp, const int64_t *d_jobs, cudaStream_t s)
+{
+        const int64_t njobs = (int64_t) hp.tjobs.size() / 4;
+        if (njobs == 0) return T3NS_OK;
+        const int grid = (int) std::min<int64_t>(njobs, 148 * 16);
+        transpose_ops_kernel<<<grid, 256, 0, s>>>(dp.ops, dp.ops_t, d_jobs, njobs);
+        T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
 }
 
 // Diagonal: diag[n](a,b,c) = sum over the terms of the (n, n) pair of
@@ -903,8 +1164,12 @@ static double tile_cost(const int *seq, int nst, const int *o, const int *ext, c
 // tensor-pipe work, among those whose intermediates fit the shared buffer;
 // fl_out receives its FLOPs and pc_out its tensor-pipe work.  Returns -1 if
 // none fits.
+// For the contraction-ordered kernel (v2) the intermediates take their padded
+// sizes, and an old block larger than psi_cap (padded) is read in place,
+// which needs a sequence that starts on memory axis 0.
 static int choose_seq(int nst, const int *o, const int *n, const int *ext, const int *nt,
-                      int w_cap, double *fl_out, double *pc_out, int seq_out[3])
+                      int w_cap, double *fl_out, double *pc_out, int seq_out[3], bool ordered = false,
+                      int psi_cap = 0)
 {
         static const int perms3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
                                          {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
@@ -916,6 +1181,13 @@ static int choose_seq(int nst, const int *o, const int *n, const int *ext, const
                 const int *seq = nst == 3 ? perms3[q] : perms2[q];
                 int64_t s1 = 0, s2 = 0;
                 const double fl = seq_cost(seq, nst, o, n, ext, nt, &s1, &s2);
+                if (ordered) {
+                        const int s0 = seq[0], q1 = seq[1], q2 = nst == 3 ? seq[2] : 3 - seq[0] - seq[1];
+                        const int64_t psz = (int64_t) v2::staged_ld(o[s0]) * o[q1] * o[q2];
+                        if (psz > psi_cap && s0 != 0) continue;
+                        s1 = (int64_t) v2::staged_ld(o[q1]) * o[q2] * ext[s0];
+                        s2 = nst == 3 ? (int64_t) v2::staged_ld(o[q2]) * ext[s0] * ext[q1] : 0;
+                }
                 if (s1 + s2 > w_cap) continue;
                 const double pc = tile_cost(seq, nst, o, ext, nt);
                 if (best < 0 || pc < bpc) { best = q; bfl = fl; bpc = pc; }
@@ -1058,6 +1330,36 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
         hp.npairs = npairs;
         hp.flops_ref = flops_ref;
 
+        // transposed operator buffer of the contraction-ordered kernel
+        {
+                hp.toff.assign(3 * hp.tasks.size(), 0);
+                hp.tjobs.clear();
+                std::unordered_map<int64_t, int64_t> tmap;
+                tmap.reserve(1 << 16);
+                int64_t tot = 0;
+                for (int nb = 0; nb < d->nblocks; ++nb)
+                        for (int t = hp.task_ptr[nb]; t < hp.task_ptr[nb + 1]; ++t) {
+                                const HeffTask &tk = hp.tasks[t];
+                                const int4 eo = hp.edims[tk.old], en = hp.edims[nb];
+                                const int o3[3] = {eo.x, eo.y, eo.z}, n3[3] = {en.x, en.y, en.z};
+                                for (int ax = 0; ax < nops; ++ax) {
+                                        auto it = tmap.find(tk.op_off[ax]);
+                                        int64_t off;
+                                        if (it == tmap.end()) {
+                                                off = tot;
+                                                tot += ((int64_t) n3[ax] * v2::op_ld(o3[ax]) + 3) & ~(int64_t) 3;
+                                                tmap.emplace(tk.op_off[ax], off);
+                                                hp.tjobs.insert(hp.tjobs.end(),
+                                                                {tk.op_off[ax], off, (int64_t) n3[ax], (int64_t) o3[ax]});
+                                        } else {
+                                                off = it->second;
+                                        }
+                                        hp.toff[3 * (size_t) t + ax] = off;
+                                }
+                        }
+                hp.opt_elems = tot;
+        }
+
         // algorithmic bytes: vectors in/out + each referenced operator block once
         {
                 std::vector<std::pair<int64_t, int64_t>> blocks;
@@ -1145,7 +1447,8 @@ int tile_plan(HostPlan &hp, int cfg)
                         for (size_t q = 0; q < ptmp.size() && ok; ++q) {
                                 int seq[3];
                                 double fl, pc;
-                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, kc.w_cap, &fl, &pc, seq) != 0) {
+                                if (choose_seq(nops, ptmp[q].eo, en, ext, nt, kc.w_cap, &fl, &pc, seq,
+                                               kc.v2 != 0, kc.psi_cap) != 0) {
                                         ok = false;
                                         break;
                                 }
@@ -1254,6 +1557,52 @@ int tile_plan(HostPlan &hp, int cfg)
         return T3NS_OK;
 }
 
+template <class Cfg, bool SPLIT>
+static int launch_v2(const DevicePlan &dp, const DeviceTiles &dt, const double *x, double *y,
+                     cudaStream_t s)
+{
+        static std::mutex mu;
+        static std::bitset<kMaxDevices> attr_set;
+        int dev = 0;
+        T3NS_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) return set_error(T3NS_E_LIMIT, "device ordinal too large");
+        {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!attr_set[dev]) {
+                        T3NS_CUDA_TRY(cudaFuncSetAttribute(heff_v2_kernel<Cfg, SPLIT>,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           (int) smem_bytes_v2<Cfg>()));
+                        attr_set[dev] = true;
+                }
+        }
+        const int share = dp.share ? std::max(1, dp.share->load(std::memory_order_relaxed)) : 1;
+        const int grid = std::max(1, dt.grid / share);
+        if constexpr (SPLIT) {
+                if (!dp.ops_t_split || !dp.toff)
+                        return set_error(T3NS_E_ARG, "matvec: the split transposed operators are not set up");
+                heff_v2_kernel<Cfg, true><<<grid, Cfg::kThreads, smem_bytes_v2<Cfg>(), s>>>(
+                        x, y, dp.ops_t_split, dp.blk_off, dp.edims, dt.units, dt.n_units, dt.pairs,
+                        dp.tasks, dp.toff, dp.counter, dp.err);
+        } else {
+                if (!dp.ops_t || !dp.toff)
+                        return set_error(T3NS_E_ARG, "matvec: the transposed operators are not set up");
+                heff_v2_kernel<Cfg, false><<<grid, Cfg::kThreads, smem_bytes_v2<Cfg>(), s>>>(
+                        x, y, dp.ops_t, dp.blk_off, dp.edims, dt.units, dt.n_units, dt.pairs, dp.tasks,
+                        dp.toff, dp.counter, dp.err);
+        }
+        T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
+}
+
+int convert_to_pairs(const double *a, float2 *b, int64_t n, cudaStream_t s)
+{
+        if (n <= 0) return T3NS_OK;
+        const int grid = (int) std::min<int64_t>((n + 255) / 256, 148 * 16);
+        split_pairs_kernel<<<grid, 256, 0, s>>>(a, b, n);
+        T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
+}
+
 template <class Cfg, class T>
 static int launch_cfg(const DevicePlan &dp, const DeviceTiles &dt, const T *x, const T *ops,
                       double *y, cudaStream_t s)
@@ -1311,18 +1660,25 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         const DeviceTiles &dt = dp.tiles[dp.active];
         if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
         const bool split = precision == T3NS_PREC_3XTF32;
-        if (split && (!dp.ops_split || !dp.x_split))
+        if (split && !kCfgs[dp.active].v2 && (!dp.ops_split || !dp.x_split))
                 return set_error(T3NS_E_ARG, "matvec: split precision is not set up on this plan");
         if (precision != T3NS_PREC_FP64 && !split)
                 return set_error(T3NS_E_ARG, "matvec: unsupported precision");
         T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
         if (launches) *launches = 0;
         if (dt.n_units == 0) return T3NS_OK;
-        if (split) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
+        // the contraction-ordered kernel splits the staged blocks itself
+        if (split && !kCfgs[dp.active].v2) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
-        static_assert(kNumCfgs == 3, "one launch branch per configuration");
+        static_assert(kNumCfgs == 5, "one launch branch per configuration");
         int rc;
-        if (split) {
+        if (dp.active == 3) {
+                rc = split ? launch_v2<CfgV2Wide, true>(dp, dt, x, y, s)
+                           : launch_v2<CfgV2Wide, false>(dp, dt, x, y, s);
+        } else if (dp.active == 4) {
+                rc = split ? launch_v2<CfgV2Large, true>(dp, dt, x, y, s)
+                           : launch_v2<CfgV2Large, false>(dp, dt, x, y, s);
+        } else if (split) {
                 const float2 *xs = dp.x_split, *os = dp.ops_split;
                 rc = dp.active == 0   ? launch_cfg<CfgLarge, float2>(dp, dt, xs, os, y, s)
                      : dp.active == 1 ? launch_cfg<CfgSmall, float2>(dp, dt, xs, os, y, s)
@@ -1333,7 +1689,7 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
                                       : launch_cfg<CfgWide, double>(dp, dt, x, dp.ops, y, s);
         }
         T3NS_TRY(rc);
-        if (launches) *launches = split ? 2 : 1;
+        if (launches) *launches = (split && !kCfgs[dp.active].v2) ? 2 : 1;
         return T3NS_OK;
 }
 

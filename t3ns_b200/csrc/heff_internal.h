@@ -51,8 +51,10 @@ struct KernelCfg {
         int psi_cap;       // staged old block
         int w_cap;         // intermediates of a group of terms
         const char *name;
+        int v2;            // 1: contraction-ordered layouts (heff_v2_kernel)
 };
-constexpr int kNumCfgs = 3;
+constexpr int kNumCfgs = 5;
+constexpr int kV2First = 3;   // configurations kV2First.. run heff_v2_kernel
 extern const KernelCfg kCfgs[kNumCfgs];
 
 // One (new, old) pair before tiling: its terms and the old block's dims.
@@ -86,6 +88,14 @@ struct HostPlan {
         TilePlan tiles[kNumCfgs];
         int64_t npairs = 0;
         double flops_ref = 0, bytes_alg = 0;
+        // transposed operator buffer of the contraction-ordered kernel: every
+        // referenced operator block row-major (new x old), rows padded with
+        // zeros to v2::op_ld(old dim), 32-byte aligned; toff[3 * task + axis]
+        // is the block's offset there, tjobs the transposition jobs
+        // {reference offset, transposed offset, rows, cols}
+        std::vector<int64_t> toff;
+        std::vector<int64_t> tjobs;
+        int64_t opt_elems = 0;
 };
 
 // Device copy of one tiling.
@@ -102,6 +112,9 @@ struct DevicePlan {
         int nblocks = 0;
         int64_t size = 0;
         double *ops = nullptr;
+        double *ops_t = nullptr;                  // transposed operators (v2 configurations)
+        float2 *ops_t_split = nullptr;            // their {hi, lo} TF32 pairs
+        int64_t *toff = nullptr;                  // their offsets per task and axis
         float2 *ops_split = nullptr;              // {hi, lo} TF32 split of the operators
         float2 *x_split = nullptr;                // {hi, lo} split of the matvec input
         int64_t *blk_off = nullptr;
@@ -129,6 +142,11 @@ int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStrea
 int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
                 int *launches);
 int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s);
+// {hi, lo} pairs of the transposed operators.
+int convert_to_pairs(const double *a, float2 *b, int64_t n, cudaStream_t s);
+// Fills dp.ops_t from dp.ops with the plan's transposition jobs.
+int build_transposed_ops(const HostPlan &hp, DevicePlan &dp, const int64_t *d_jobs,
+                         cudaStream_t s);
 int launch_heff_diag(const DevicePlan &dp, double *diag, cudaStream_t s);
 
 }  // namespace t3ns

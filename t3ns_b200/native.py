@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(_HERE, "_lib")
 
 T3NS_PREC_FP64 = 0
-T3NS_NUM_CONFIGS = 3   # kernel configurations of the matvec
+T3NS_NUM_CONFIGS = 5   # kernel configurations of the matvec (3, 4: FP64 only)
 T3NS_PREC_3XTF32 = 1
 T3NS_PREC_BF16X3 = 2
 
@@ -94,6 +94,7 @@ def load(path: str | None = None):
     lib.t3ns_heff_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.t3ns_heff_get_stats.argtypes = [C.c_void_p, C.POINTER(HeffStats)]
     lib.t3ns_heff_last_launches.argtypes = [C.c_void_p]
+    lib.t3ns_heff_check_status.argtypes = [C.c_void_p, C.c_void_p]
     lib.t3ns_heff_destroy.argtypes = [C.c_void_p]
     lib.t3ns_heff_destroy.restype = None
     lib.t3ns_last_error.restype = C.c_char_p

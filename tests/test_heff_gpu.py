@@ -96,7 +96,7 @@ def test_davidson_energy_matches_reference(path, torch_cuda):
     plan.close()
 
 
-@pytest.mark.parametrize("config", [0, 1, 2])
+@pytest.mark.parametrize("config", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("path", STEPS[::3], ids=lambda p: "/".join(p.split("/")[-2:]))
 def test_matvec_every_kernel_config(path, config, torch_cuda):
     """Every kernel configuration (its own tiling) matches the reference."""
@@ -115,12 +115,13 @@ def test_autotune_picks_fastest_and_caches(torch_cuda):
     s = read_step(STEPS[-1])
     plan = HeffPlan(StepDesc(s))
     ms = plan.autotune(reps=2, force=True)
-    assert all(t > 0 for t in ms)
+    assert all(t > 0 for t in ms)        # FP64: every configuration is timed
     assert plan.config() == int(np.argmin(ms))
     assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= MATVEC_RTOL
     again = HeffPlan(StepDesc(s))
     assert again.config() == plan.config()
-    assert again.autotune(reps=1, force=False) == [0.0] * 3   # bucket known: not re-timed
+    from t3ns_b200.native import T3NS_NUM_CONFIGS
+    assert again.autotune(reps=1, force=False) == [0.0] * T3NS_NUM_CONFIGS   # bucket known: not re-timed
     again.close()
     plan.close()
 
@@ -133,7 +134,7 @@ def test_autotune_picks_fastest_and_caches(torch_cuda):
 SPLIT_RTOL = 5e-6
 
 
-@pytest.mark.parametrize("config", [0, 1, 2])
+@pytest.mark.parametrize("config", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("path", STEPS[::2], ids=lambda p: "/".join(p.split("/")[-2:]))
 def test_split_precision_matvec_error(path, config, torch_cuda):
     from t3ns_b200.native import T3NS_PREC_3XTF32
@@ -143,7 +144,9 @@ def test_split_precision_matvec_error(path, config, torch_cuda):
     for v in range(2):
         err = _rel(plan.matvec_host(s[f"x{v}"]), s[f"y{v}"])
         assert err <= SPLIT_RTOL, err
-    assert plan.last_launches() == 2      # FP32 conversion of x + the matvec
+    # configurations 0-2: conversion of x to pairs + the matvec; 3, 4 split
+    # the staged blocks inside the matvec
+    assert plan.last_launches() == (2 if config < 3 else 1)
     plan.close()
 
 
@@ -204,3 +207,39 @@ def test_davidson_graphs_through_deflation(torch_cuda):
     plan.close()
     assert ret == 0 and info["iterations"] > 4
     assert abs(e - float(s["eig.energy"][0])) <= ENERGY_TOL
+
+
+@pytest.mark.parametrize("path", STEPS[::4], ids=lambda p: "/".join(p.split("/")[-2:]))
+def test_device_matvec_status_is_clean(path, torch_cuda):
+    """t3ns_heff_check_status after device-pointer matvecs in every
+    configuration reports no kernel error."""
+    import ctypes as C
+    torch = torch_cuda
+    s = read_step(path)
+    plan = HeffPlan(StepDesc(s))
+    x = torch.from_numpy(s["x0"]).cuda()
+    y = torch.empty_like(x)
+    st = torch.cuda.current_stream().cuda_stream
+    for config in range(5):
+        plan.set_config(config)
+        plan.matvec_device(x.data_ptr(), y.data_ptr(), st)
+        assert plan.lib.t3ns_heff_check_status(plan.h, C.c_void_p(st)) == 0
+        assert _rel(y.cpu().numpy(), s["y0"]) <= MATVEC_RTOL
+    plan.close()
+
+
+def test_ordered_configs_switch_precision(torch_cuda):
+    """A plan on a contraction-ordered configuration switches between FP64
+    and split precision in place (the {hi, lo} operator pairs are built on
+    the first switch) and stays within each precision's tolerance."""
+    from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_FP64
+    s = read_step(golden_steps()[0])
+    plan = HeffPlan(StepDesc(s))
+    plan.set_config(3)
+    assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= MATVEC_RTOL
+    plan.set_precision(T3NS_PREC_3XTF32)
+    assert plan.config() == 3
+    assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= SPLIT_RTOL
+    plan.set_precision(T3NS_PREC_FP64)
+    assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= MATVEC_RTOL
+    plan.close()

@@ -45,7 +45,7 @@ def d512(cuda):
     return s, StepDesc(s)
 
 
-@pytest.mark.parametrize("config", [0, 1, 2])
+@pytest.mark.parametrize("config", [0, 1, 2, 3, 4])
 def test_d512_matvec_matches_reference(d512, config):
     s, d = d512
     plan = HeffPlan(d)
@@ -63,7 +63,7 @@ def test_d512_diagonal_matches_reference(d512):
     plan.close()
 
 
-@pytest.mark.parametrize("config", [0, 1, 2])
+@pytest.mark.parametrize("config", [0, 1, 2, 3, 4])
 def test_d512_split_precision_error(d512, config):
     s, d = d512
     plan = HeffPlan(d, T3NS_PREC_3XTF32)
@@ -85,7 +85,7 @@ def test_workload_matches_oracle_on_sampled_blocks(path, cuda):
     off = s["beginblock"].astype(np.int64)
     sel = np.concatenate([np.arange(off[b], off[b + 1]) for b in blocks])
     plan = HeffPlan(d)
-    for config in range(3):
+    for config in range(5):
         plan.set_config(config)
         y = plan.matvec_host(x)
         assert np.isfinite(y).all()

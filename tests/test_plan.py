@@ -20,7 +20,7 @@ def _check(s, plan, blocks):
     assert fl[1] >= fl[0] * (1 - 1e-12)   # executed FLOPs never undercut the reference's
 
 
-CONFIGS = (0, 1, 2)   # the engine's kernel configurations (large, small and mid-size tiles)
+CONFIGS = (0, 1, 2, 3, 4)   # the engine's kernel configurations (3, 4: contraction-ordered)
 
 
 @pytest.mark.parametrize("config", CONFIGS)
