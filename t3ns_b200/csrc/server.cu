@@ -75,10 +75,10 @@ int64_t estimate_solve_bytes(const t3ns_heff_desc *d, int precision, int max_vec
                 tasks += d->MPOc_beg[d->combo_mpo[c] + 1] - d->MPOc_beg[d->combo_mpo[c]];
         const bool split = precision == T3NS_PREC_3XTF32;
         int64_t b = op_elems * (split ? 16 : 8);               // FP64 (+ {hi, lo} pairs)
-        // FP64 plans also hold the transposed operators of the contraction-
-        // ordered kernel (rows padded to 4: at most 4 more doubles a row, so
-        // bounded here by twice the operators) and their offsets per term
-        if (!split) b += op_elems * 16 + tasks * 3 * (int64_t) sizeof(int64_t);
+        // the transposed operators of the contraction-ordered configurations
+        // (rows padded to 4: bounded here by twice the operators; their {hi, lo}
+        // pairs too in split precision) and their offsets per term
+        b += op_elems * (split ? 32 : 16) + tasks * 3 * (int64_t) sizeof(int64_t);
         b += tasks * (int64_t) sizeof(HeffTask);
         b += kNumCfgs * npairs * (int64_t) (sizeof(HeffPair) + 4 * sizeof(HeffUnit));
         b += n * (16 + (split ? 8 : 0));                      // plan staging (+ split input)
