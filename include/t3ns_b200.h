@@ -274,6 +274,45 @@ typedef struct {
 int t3ns_bupdate_host(const t3ns_bupdate_desc *d, const double *t_tel, const double *o1_tel,
                       const double *o2_tel, double *new_tel);
 
+/* Sum of unique renormalised operators into a new set, then removal of the
+ * blocks whose elements are all below 1e-20 in magnitude (reference
+ * sum_unique_rOperators, src/rOperators_init.c:228-265, with
+ * kick_zero_blocks, src/sparseblocks.c:73-107).  New operator k gets, for
+ * each instruction writing it (in instruction order), pref times the unique
+ * operator at element offset instr_src; its block layout before removal is
+ * begin[begin_ptr[k] .. begin_ptr[k+1]) (starting at 0, the last entry its
+ * size) and its elements sit at new_base[k] in the unsummed layout
+ * (new_base[k+1] - new_base[k] = its size). */
+typedef struct {
+        int nnew;
+        const int64_t *begin_ptr;   /* [nnew + 1] into begin                  */
+        const int *begin;           /* block begin offsets before removal     */
+        const int64_t *new_base;    /* [nnew + 1]                             */
+        const int *instr_ptr;       /* [nnew + 1] CSR into the instructions   */
+        const int64_t *instr_src;   /* [ninstr] unique operator element base  */
+        const double *instr_pref;   /* [ninstr]                               */
+        int64_t unique_elems;       /* size of unique_tel (standalone call)   */
+} t3ns_sumunique_desc;
+
+/* Outputs of the sums: new_tel (new_base[nnew] doubles at most) receives the
+ * kept blocks of every new operator back to back, operator k from
+ * out_base[k] (out_base has nnew + 1 entries); new_begin (shaped like
+ * begin) the block begin offsets after removal.  Host arrays. */
+int t3ns_sum_unique_host(const t3ns_sumunique_desc *s, const double *unique_tel, double *new_tel,
+                         int *new_begin, int64_t *out_base);
+
+/* The site-operator append (t3ns_scalecopy_host) and the branching update
+ * (t3ns_bupdate_host) followed by the sum on the device: the unique
+ * operators never leave the GPU, only the summed set is downloaded
+ * (reference rOperators_append_phys, src/rOperators_pUpdate.c:665-673, and
+ * update_rOperators_branching, src/rOperators_bUpdate.c:229-248, which end
+ * in sum_unique_rOperators). */
+int t3ns_scalecopy_sum_host(const t3ns_scalecopy_desc *d, const t3ns_sumunique_desc *s,
+                            const double *src, double *new_tel, int *new_begin, int64_t *out_base);
+int t3ns_bupdate_sum_host(const t3ns_bupdate_desc *d, const t3ns_sumunique_desc *s,
+                          const double *t_tel, const double *o1_tel, const double *o2_tel,
+                          double *new_tel, int *new_begin, int64_t *out_base);
+
 /* Dense FP64 factorisations of one symmetry sector of the site-tensor
  * decomposition, on host column-major arrays, with LAPACK's argument
  * meaning.  They replace the reference's LAPACKE_dgesdd ('S' and 'N'),

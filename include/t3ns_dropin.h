@@ -71,6 +71,13 @@ void update_rOperators_physical(struct rOperators *rops, const struct siteTensor
  * operators of the next physical site appended. */
 void rOperators_append_phys(struct rOperators *newrops, const struct rOperators *oldrops);
 
+/* Replaces sum_unique_rOperators, reference include/rOperators.h:159-160,
+ * src/rOperators_init.c:228-265: the new set summed from the unique
+ * operators `ur` with the instruction set, zero blocks removed (the sums on
+ * the GPU).  The drop-in's own updates sum on the device without this call. */
+struct instructionset;
+struct rOperators sum_unique_rOperators(const struct rOperators *ur, const struct instructionset *set);
+
 /* Replaces update_rOperators_branching, reference include/rOperators.h:289-291,
  * src/rOperators_bUpdate.c:229-248: *newops receives the set on the free bond
  * of the branching tensor tens, built from Operator[0] and Operator[1]. */

@@ -401,6 +401,54 @@ void update_rOperators_physical(struct rOperators *rops, const struct siteTensor
         }
 }
 
+/* --check-dropin LIB: every rOperators_append_phys call of the sweep also
+ * runs the drop-in's (LIB loaded privately, so its symbols do not replace
+ * the reference's) on the same input, and the two new sets are compared:
+ * "CHECK_APPEND <call> <diff>" with diff the largest element difference
+ * relative to the largest reference element, or -1 when the block
+ * structures differ (operator count, sectors, surviving blocks). */
+static const char *opt_check_dropin;
+static int opt_check_count;
+
+static double compare_rops(const struct rOperators *a, const struct rOperators *b)
+{
+        if (a->nrops != b->nrops || a->nrhss != b->nrhss || a->bond != b->bond ||
+            a->is_left != b->is_left || a->P_operator != b->P_operator)
+                return -1;
+        double scale = 0, worst = 0;
+        for (int i = 0; i < a->nrops; ++i) {
+                if (a->hss_of_ops[i] != b->hss_of_ops[i]) return -1;
+                const int nb = nblocks_in_operator(a, i);
+                for (int q = 0; q <= nb; ++q)
+                        if (a->operators[i].beginblock[q] != b->operators[i].beginblock[q]) return -1;
+                for (int j = 0; j < a->operators[i].beginblock[nb]; ++j) {
+                        const double x = a->operators[i].tel[j], y = b->operators[i].tel[j];
+                        if (fabs(x) > scale) scale = fabs(x);
+                        if (fabs(x - y) > worst) worst = fabs(x - y);
+                }
+        }
+        return scale > 0 ? worst / scale : worst;
+}
+
+typedef void (*append_fn)(struct rOperators *, const struct rOperators *);
+void rOperators_append_phys(struct rOperators *newrops, const struct rOperators *oldrops)
+{
+        static append_fn real, mine;
+        if (!real) real = (append_fn) dlsym(RTLD_NEXT, "rOperators_append_phys");
+        real(newrops, oldrops);
+        if (!opt_check_dropin) return;
+        if (!mine) {
+                void *h = dlopen(opt_check_dropin, RTLD_NOW | RTLD_LOCAL);
+                if (!h) { fprintf(stderr, "%s\n", dlerror()); exit(EXIT_FAILURE); }
+                mine = (append_fn) dlsym(h, "rOperators_append_phys");
+                if (!mine) { fprintf(stderr, "no rOperators_append_phys in %s\n", opt_check_dropin); exit(EXIT_FAILURE); }
+        }
+        struct rOperators other;
+        mine(&other, oldrops);
+        printf("CHECK_APPEND %d %.3e\n", opt_check_count++, compare_rops(newrops, &other));
+        destroy_rOperators(&other);
+}
+
 /* Captures the reference's branching update the same way: both input sets
  * (ops0, ops1), the branching tensor, the product's compiled schedule and the
  * reference's output (ops2).  Interposes update_rOperators_branching
@@ -661,6 +709,9 @@ int main(int argc, char **argv)
                 else if (!strcmp(a, "--capture-stop")) { opt_capture_stop = 1; }
                 else if (!strcmp(a, "--capture-noeig")) { opt_capture_noeig = 1; }
                 else if (!strcmp(a, "--schedule-lib") && v) { opt_schedule_lib = v; ++i; }
+#ifndef T3NS_RUN_DROPIN
+                else if (!strcmp(a, "--check-dropin") && v) { opt_check_dropin = v; ++i; }
+#endif
                 else if (!strcmp(a, "--capture-pupdate") && v) { opt_capture_pupdate = v; ++i; }
                 else if (!strcmp(a, "--capture-pupdate-limit") && v) { opt_pupdate_limit = atoi(v); ++i; }
                 else if (!strcmp(a, "--capture-dense") && v) { opt_capture_dense = v; ++i; }

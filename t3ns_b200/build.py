@@ -57,7 +57,8 @@ def build_engine(force: bool = False) -> str:
 
 
 SHIM_INCLUDE = os.path.join(ROOT, "oracle", "shim")
-DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c", "bupdate_dropin.c", "dense_dropin.c"]
+DROPIN_SOURCES = ["heff_dropin.c", "pupdate_dropin.c", "bupdate_dropin.c", "sum_dropin.c",
+                  "dense_dropin.c"]
 
 
 def reference_checkout(reference: str | None = None) -> str:
@@ -79,7 +80,9 @@ def build_dropin(force: bool = False, reference: str | None = None):
     engine = build_engine()
     out = os.path.join(LIBDIR, "libt3ns_dropin.so")
     srcs = [os.path.join(CSRC, "dropin", f) for f in DROPIN_SOURCES]
-    if force or _stale(out, srcs + [engine, os.path.join(INCLUDE, "t3ns_b200.h")]):
+    hdrs = [os.path.join(CSRC, "dropin", f) for f in os.listdir(os.path.join(CSRC, "dropin"))
+            if f.endswith(".h")]
+    if force or _stale(out, srcs + hdrs + [engine, os.path.join(INCLUDE, "t3ns_b200.h")]):
         _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu11", "-w", "-DMAX_SYMMETRIES=5",
               "-DNDEBUG", "-I", ref_include, "-I", SHIM_INCLUDE, "-I", INCLUDE,
               "-o", out, *srcs, "-L", LIBDIR, "-l:libt3ns_b200.so", "-Wl,-rpath,$ORIGIN",

@@ -59,6 +59,8 @@ static std::tuple<int, int, int, int> size_bucket(const HostPlan &hp, int precis
         return {lg((double) hp.size), lg((double) maxblk), lg(hp.flops_ref), precision};
 }
 
+static int check_device_error(t3ns_heff *h, cudaStream_t s = nullptr);
+
 // Transposed operators of the contraction-ordered configurations (built on
 // the device from the resident operators, on first use).
 static int setup_transposed(t3ns_heff *h)
@@ -74,9 +76,15 @@ static int setup_transposed(t3ns_heff *h)
                 const cudaError_t e = cudaMemcpy(d_jobs, hp.tjobs.data(), sizeof(int64_t) * hp.tjobs.size(),
                                                  cudaMemcpyHostToDevice);
                 int rc = e == cudaSuccess ? build_transposed_ops(hp, dp, d_jobs, h->stream)
-                                          : set_error(T3NS_E_CUDA, "transposed operators: upload");
-                if (rc == T3NS_OK && cudaStreamSynchronize(h->stream) != cudaSuccess)
-                        rc = set_error(T3NS_E_CUDA, "transposed operators: kernel");
+                                          : set_error(T3NS_E_CUDA, std::string("transposed operators: upload: ") +
+                                                                       cudaGetErrorString(e));
+                if (rc == T3NS_OK) {
+                        const cudaError_t se = cudaStreamSynchronize(h->stream);
+                        if (se != cudaSuccess)
+                                rc = set_error(T3NS_E_CUDA, std::string("transposed operators: kernel: ") +
+                                                                    cudaGetErrorString(se));
+                }
+                if (rc == T3NS_OK) rc = check_device_error(h);
                 cudaFree(d_jobs);
                 T3NS_TRY(rc);
         }
@@ -170,20 +178,22 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
                 auto it = g_tune_cache.find(size_bucket(hp, precision));
                 if (it != g_tune_cache.end()) cfg = it->second;
         }
-        T3NS_TRY(upload_tiles(h, cfg));
-        dp.active = cfg;
+        // status word, counter and stream first: the tiling of a cached
+        // configuration may already launch set-up kernels
         T3NS_TRY(dev_alloc(h, &dp.counter, 1));
         T3NS_TRY(dev_alloc(h, &dp.err, 1));
         T3NS_CUDA_TRY(cudaMemset(dp.err, 0, sizeof(int)));
         T3NS_TRY(dev_alloc(h, &h->stage_x, (size_t) hp.size));
         T3NS_TRY(dev_alloc(h, &h->stage_y, (size_t) hp.size));
         T3NS_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        T3NS_TRY(upload_tiles(h, cfg));
+        dp.active = cfg;
         return setup_precision(h, precision);
 }
 
 // Reads the kernel's error status after the work on stream s (the plan's
 // own stream when s is null): the copy is ordered after that work.
-static int check_device_error(t3ns_heff *h, cudaStream_t s = nullptr)
+static int check_device_error(t3ns_heff *h, cudaStream_t s)
 {
         if (!s) s = h->stream;
         int err = 0;
@@ -407,6 +417,9 @@ int t3ns_heff_plan_dump_config(const t3ns_heff_desc *desc, int config, const cha
         put("plan.op_off", 2, (int64_t) offs.size(), offs.data());
         put("plan.pref", 3, (int64_t) prefs.size(), prefs.data());
         put("plan.flops", 3, 2, std::vector<double>{hp.flops_ref, tp.flops_exec}.data());
+        put("plan.tjobs", 2, (int64_t) hp.tjobs.size(), hp.tjobs.data());
+        put("plan.toff", 2, (int64_t) hp.toff.size(), hp.toff.data());
+        put("plan.elems", 2, 2, std::vector<int64_t>{hp.op_elems, hp.opt_elems}.data());
         fclose(f);
         return T3NS_OK;
 }

@@ -587,9 +587,11 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                         return rc;
                 }
                 m = deflate ? keep : m + 1;
-                if (cudaStreamSynchronize(s) != cudaSuccess) {
+                const cudaError_t se = cudaStreamSynchronize(s);
+                if (se != cudaSuccess) {
                         release();
-                        return set_error(T3NS_E_CUDA, "davidson: iteration failed");
+                        return set_error(T3NS_E_CUDA, std::string("davidson: iteration failed: ") +
+                                                              cudaGetErrorString(se));
                 }
                 int st = 0;
                 if (mv_err) {

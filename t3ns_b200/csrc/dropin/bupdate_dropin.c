@@ -48,7 +48,7 @@
 #include "symsecs.h"
 
 #include "t3ns_b200.h"
-#include "dropin_util.h"
+#include "dropin_sum.h"
 
 enum { BU_BRA = 0, BU_KET = 1, BU_MPO = 2 };
 
@@ -314,17 +314,19 @@ void update_rOperators_branching(struct rOperators *newops, const struct rOperat
         bu_desc(&S, Operator, tens, &d);
         double *o1 = dropin_gather(&Operator[0], S.base1);
         double *o2 = dropin_gather(&Operator[1], S.base2);
-        double *nw = safe_malloc(d.new_elems + 1, double);
-        if (t3ns_bupdate_host(&d, tens->blocks.tel, o1, o2, nw) != T3NS_OK) {
+        /* the unique operators stay on the device and are summed there
+         * (sum_unique_rOperators, src/rOperators_init.c:228-265) */
+        struct dropin_sum su;
+        dropin_sum_build(&su, &S.uo, &S.set, S.ubase, newops);
+        if (t3ns_bupdate_sum_host(&d, &su.d, tens->blocks.tel, o1, o2, su.new_tel, su.new_begin,
+                                  su.out_base) != T3NS_OK) {
                 fprintf(stderr, "t3ns drop-in: update_rOperators_branching: %s\n", t3ns_last_error());
                 exit(EXIT_FAILURE);
         }
-        dropin_scatter(&S.uo, S.ubase, nw);
-        *newops = sum_unique_rOperators(&S.uo, &S.set);
+        dropin_sum_finish(&su, newops);
         destroy_rOperators(&S.uo);
         safe_free(o1);
         safe_free(o2);
-        safe_free(nw);
         bu_free(&S);
 }
 

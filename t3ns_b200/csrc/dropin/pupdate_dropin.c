@@ -35,7 +35,7 @@
 #include "symsecs.h"
 
 #include "t3ns_b200.h"
-#include "dropin_util.h"
+#include "dropin_sum.h"
 
 struct pu_sched {
         struct rOperators ur;        /* updated operators (structure + calloc'd tel) */
@@ -381,18 +381,20 @@ void rOperators_append_phys(struct rOperators *newrops, const struct rOperators 
         }
 
         double *src_tel = dropin_gather(or, obase);
-        double *dst_tel = safe_malloc(ubase[ur.nrops] + 1, double);
         t3ns_scalecopy_desc d = {(int) scl.n, dst.a, src.a, len.a, scl.a, obase[or->nrops],
                                  ubase[ur.nrops]};
-        if (t3ns_scalecopy_host(&d, src_tel, dst_tel) != T3NS_OK) {
+        /* the scaled copies (the unique operators) are summed on the device
+         * (sum_unique_rOperators, src/rOperators_init.c:228-265) */
+        struct dropin_sum su;
+        dropin_sum_build(&su, &ur, &set, ubase, newrops);
+        if (t3ns_scalecopy_sum_host(&d, &su.d, src_tel, su.new_tel, su.new_begin, su.out_base) !=
+            T3NS_OK) {
                 fprintf(stderr, "t3ns drop-in: rOperators_append_phys: %s\n", t3ns_last_error());
                 exit(EXIT_FAILURE);
         }
-        dropin_scatter(&ur, ubase, dst_tel);
-        *newrops = sum_unique_rOperators(&ur, &set);
+        dropin_sum_finish(&su, newrops);
         destroy_rOperators(&ur);   /* `set` is the reference's cached set: not ours to free */
         safe_free(src_tel);
-        safe_free(dst_tel);
         safe_free(obase);
         safe_free(ubase);
         safe_free(ci);

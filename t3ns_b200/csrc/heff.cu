@@ -1036,13 +1036,21 @@ __global__ void split_pairs_kernel(const double *__restrict__ a, float2 *__restr
 // cols) column-major block at ops[src] -> row-major at opt[dst] with rows of
 // v2::op_ld(cols) doubles (the padding zeroed).
 __global__ void transpose_ops_kernel(const double *__restrict__ ops, double *__restrict__ opt,
-                                     const int64_t *__restrict__ jobs, int64_t njobs)
+                                     const int64_t *__restrict__ jobs, int64_t njobs, int64_t n_ops,
+                                     int64_t n_opt, int *err)
 {
         for (int64_t j = blockIdx.x; j < njobs; j += gridDim.x) {
                 const int64_t src = jobs[4 * j], dst = jobs[4 * j + 1];
                 const int rows = (int) jobs[4 * j + 2], cols = (int) jobs[4 * j + 3];
                 const int ld = v2::op_ld(cols);
                 const int n = rows * ld;
+                // the host checks every job before the launch; a job out of
+                // range is recorded and skipped here all the same
+                if (rows < 0 || cols < 0 || src < 0 || src + (int64_t) rows * cols > n_ops || dst < 0 ||
+                    dst + n > n_opt) {
+                        if (threadIdx.x == 0) atomicExch(err, 5);
+                        continue;
+                }
                 for (int e = threadIdx.x; e < n; e += blockDim.x) {
                         const int r = e / ld, k = e - r * ld;
                         opt[dst + e] = k < cols ? ops[src + r + (int64_t) k * rows] : 0.0;
@@ -1054,8 +1062,16 @@ int build_transposed_ops(const HostPlan &hp, DevicePlan &dp, const int64_t *d_jo
 {
         const int64_t njobs = (int64_t) hp.tjobs.size() / 4;
         if (njobs == 0) return T3NS_OK;
+        for (int64_t j = 0; j < njobs; ++j) {
+                const int64_t *jb = &hp.tjobs[4 * j];
+                if (jb[2] < 0 || jb[3] < 0 || jb[0] < 0 || jb[0] + jb[2] * jb[3] > hp.op_elems ||
+                    jb[1] < 0 || jb[1] + jb[2] * v2::op_ld((int) jb[3]) > hp.opt_elems)
+                        return set_error(T3NS_E_ARG, "transposed operators: job " + std::to_string(j) +
+                                                             " out of range");
+        }
         const int grid = (int) std::min<int64_t>(njobs, 148 * 16);
-        transpose_ops_kernel<<<grid, 256, 0, s>>>(dp.ops, dp.ops_t, d_jobs, njobs);
+        transpose_ops_kernel<<<grid, 256, 0, s>>>(dp.ops, dp.ops_t, d_jobs, njobs, hp.op_elems,
+                                                  hp.opt_elems, dp.err);
         T3NS_CUDA_TRY(cudaGetLastError());
         return T3NS_OK;
 }

@@ -172,6 +172,58 @@ bupdate_kernel(int3 ax, int nunits, const int *__restrict__ unit_ptr,
         }
 }
 
+// Sum of unique operators (reference sum_unique_rOperators,
+// src/rOperators_init.c:228-265): new operator k, element j =
+// sum over the instructions writing k, in instruction order, of
+// pref * unique[src + j] (fused multiply-adds from zero).  One CTA per new
+// operator (grid-stride), threads over its elements.
+__global__ void sum_unique_kernel(int nnew, const int64_t *__restrict__ new_base,
+                                  const int *__restrict__ instr_ptr,
+                                  const int64_t *__restrict__ instr_src,
+                                  const double *__restrict__ instr_pref,
+                                  const double *__restrict__ U, double *__restrict__ NEW)
+{
+        for (int k = blockIdx.x; k < nnew; k += gridDim.x) {
+                const int64_t b = new_base[k], n = new_base[k + 1] - b;
+                const int i0 = instr_ptr[k], i1 = instr_ptr[k + 1];
+                for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+                        double acc = 0.0;
+                        for (int i = i0; i < i1; ++i) acc = fma(instr_pref[i], U[instr_src[i] + j], acc);
+                        NEW[b + j] = acc;
+                }
+        }
+}
+
+// Zero-block test of kick_zero_blocks (src/sparseblocks.c:73-107): a block
+// is kept when one of its elements has magnitude 1e-20 or more
+// (COMPARE_ELEMENT_TO_ZERO, include/macros.h:24).  Block q of the flattened
+// list spans NEW[off[q], off[q] + len[q]); one warp per block.
+__global__ void nonzero_blocks_kernel(int64_t nblocks, const int64_t *__restrict__ off,
+                                      const int *__restrict__ len, const double *__restrict__ NEW,
+                                      int *__restrict__ keep)
+{
+        const int lane = threadIdx.x & 31;
+        const int64_t w0 = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t) gridDim.x * blockDim.x) >> 5;
+        for (int64_t q = w0; q < nblocks; q += nw) {
+                const double *p = NEW + off[q];
+                bool nz = false;
+                for (int j = lane; j < len[q] && !nz; j += 32) nz = fabs(p[j]) >= 1e-20;
+                nz = __any_sync(0xffffffffu, nz);
+                if (lane == 0) keep[q] = nz ? 1 : 0;
+        }
+}
+
+// Gathers the kept blocks: entry e copies len[e] elements from src_off[e]
+// to dst_off[e] (one CTA per entry, grid-stride).
+__global__ void gather_blocks_kernel(int64_t n, const int64_t *__restrict__ src_off,
+                                     const int64_t *__restrict__ dst_off, const int *__restrict__ len,
+                                     const double *__restrict__ SRC, double *__restrict__ DST)
+{
+        for (int64_t e = blockIdx.x; e < n; e += gridDim.x)
+                for (int j = threadIdx.x; j < len[e]; j += blockDim.x) DST[dst_off[e] + j] = SRC[src_off[e] + j];
+}
+
 // The arrays of one call laid out in the thread's workspace: inputs first
 // (staged in the pinned buffer at their device offsets and uploaded with one
 // copy), then the zero-initialised outputs, then the scratch.
@@ -222,6 +274,151 @@ template <class T>
 T *at(const ThreadWork &tw, size_t off)
 {
         return reinterpret_cast<T *>(tw.dev + off);
+}
+
+// Checks a sum-of-unique-operators descriptor against the unique buffer it
+// reads; returns the number of blocks of the new set.
+int check_sum_desc(const t3ns_sumunique_desc *s, int64_t unique_elems, int64_t *nblocks_out)
+{
+        if (!s || s->nnew < 0) return set_error(T3NS_E_ARG, "sum_unique: bad descriptor");
+        int64_t nbl = 0;
+        for (int k = 0; k < s->nnew; ++k) {
+                const int64_t b0 = s->begin_ptr[k], b1 = s->begin_ptr[k + 1];
+                if (b1 <= b0) return set_error(T3NS_E_ARG, "sum_unique: empty begin array");
+                const int *bb = s->begin + b0;
+                if (bb[0] != 0) return set_error(T3NS_E_ARG, "sum_unique: begin array must start at 0");
+                for (int64_t q = 1; q < b1 - b0; ++q)
+                        if (bb[q] < bb[q - 1]) return set_error(T3NS_E_ARG, "sum_unique: begin array decreases");
+                if (s->new_base[k + 1] - s->new_base[k] != bb[b1 - b0 - 1])
+                        return set_error(T3NS_E_ARG, "sum_unique: operator size != its last begin offset");
+                const int n = bb[b1 - b0 - 1];
+                for (int i = s->instr_ptr[k]; i < s->instr_ptr[k + 1]; ++i)
+                        if (s->instr_src[i] < 0 || s->instr_src[i] + n > unique_elems)
+                                return set_error(T3NS_E_ARG, "sum_unique: unique operator out of range");
+                nbl += b1 - b0 - 1;
+        }
+        *nblocks_out = nbl;
+        return T3NS_OK;
+}
+
+// Layout of the arrays of the sum on the device, after the call's own.
+struct SumLayout {
+        size_t nbase, iptr, isrc, ipref, bptr, bbeg;   // inputs
+        size_t sum, qoff, qlen, keep, goff_src, goff_dst, glen, out;   // work and output
+};
+
+// Adds the sum's inputs to the call's layout (before its in_end) ...
+void sum_inputs(CallLayout &L, SumLayout &S, const t3ns_sumunique_desc *s)
+{
+        const int ninstr = s->nnew ? s->instr_ptr[s->nnew] : 0;
+        S.nbase = L.input(s->new_base, s->nnew + 1);
+        S.iptr = L.input(s->instr_ptr, s->nnew + 1);
+        S.isrc = L.input(s->instr_src, ninstr);
+        S.ipref = L.input(s->instr_pref, ninstr);
+        S.bptr = L.input(s->begin_ptr, s->nnew + 1);
+        S.bbeg = L.input(s->begin, s->nnew ? s->begin_ptr[s->nnew] : 0);
+}
+
+// ... and its work arrays after the call's outputs.
+void sum_work(CallLayout &L, SumLayout &S, const t3ns_sumunique_desc *s, int64_t nbl)
+{
+        const int64_t nsum = s->new_base[s->nnew];
+        S.sum = L.c.take<double>(nsum);
+        S.qoff = L.c.take<int64_t>(nbl);
+        S.qlen = L.c.take<int>(nbl);
+        S.keep = L.c.take<int>(nbl);
+        S.goff_src = L.c.take<int64_t>(nbl);
+        S.goff_dst = L.c.take<int64_t>(nbl);
+        S.glen = L.c.take<int>(nbl);
+        S.out = L.c.take<double>(nsum);
+}
+
+// Runs the sum of the unique operators at d_unique (device) into the work
+// arrays, removes the zero blocks and downloads the kept blocks of every new
+// operator back to back (operator k from out_base[k]) with their begin
+// offsets after removal (new_begin, shaped like s->begin).  The block list
+// and the gather list go through the pinned buffer at host offset hoff.
+int sum_run(ThreadWork &tw, const SumLayout &S, const t3ns_sumunique_desc *s, int64_t nbl,
+            const double *d_unique, double *new_tel, int *new_begin, int64_t *out_base)
+{
+        cudaStream_t st = tw.st;
+        const int nnew = s->nnew;
+        if (nnew == 0) {
+                if (out_base) out_base[0] = 0;
+                return T3NS_OK;
+        }
+        // flattened block list: offset and length of every block before removal
+        std::vector<int64_t> qoff((size_t) nbl);
+        std::vector<int> qlen((size_t) nbl);
+        {
+                int64_t q = 0;
+                for (int k = 0; k < nnew; ++k) {
+                        const int *bb = s->begin + s->begin_ptr[k];
+                        const int nb = (int) (s->begin_ptr[k + 1] - s->begin_ptr[k] - 1);
+                        for (int b = 0; b < nb; ++b, ++q) {
+                                qoff[q] = s->new_base[k] + bb[b];
+                                qlen[q] = bb[b + 1] - bb[b];
+                        }
+                }
+        }
+        int *hkeep = reinterpret_cast<int *>(tw.host);
+        T3NS_CUDA_TRY(cudaMemcpyAsync(tw.dev + S.qoff, qoff.data(), sizeof(int64_t) * nbl,
+                                      cudaMemcpyHostToDevice, st));
+        T3NS_CUDA_TRY(cudaMemcpyAsync(tw.dev + S.qlen, qlen.data(), sizeof(int) * nbl,
+                                      cudaMemcpyHostToDevice, st));
+        sum_unique_kernel<<<std::min(nnew, 148 * 8), 256, 0, st>>>(
+                nnew, at<int64_t>(tw, S.nbase), at<int>(tw, S.iptr), at<int64_t>(tw, S.isrc),
+                at<double>(tw, S.ipref), d_unique, at<double>(tw, S.sum));
+        T3NS_CUDA_TRY(cudaGetLastError());
+        if (nbl > 0) {
+                const int grid = (int) std::min<int64_t>((nbl + 7) / 8, 148 * 16);
+                nonzero_blocks_kernel<<<grid, 256, 0, st>>>(nbl, at<int64_t>(tw, S.qoff), at<int>(tw, S.qlen),
+                                                           at<double>(tw, S.sum), at<int>(tw, S.keep));
+                T3NS_CUDA_TRY(cudaGetLastError());
+                T3NS_CUDA_TRY(cudaMemcpyAsync(hkeep, tw.dev + S.keep, sizeof(int) * nbl,
+                                              cudaMemcpyDeviceToHost, st));
+        }
+        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
+        // begin offsets after removal and the gather list of the kept blocks
+        std::vector<int64_t> gsrc, gdst;
+        std::vector<int> glen;
+        int64_t q = 0, tot = 0;
+        for (int k = 0; k < nnew; ++k) {
+                const int *bb = s->begin + s->begin_ptr[k];
+                int *nbb = new_begin + s->begin_ptr[k];
+                const int nb = (int) (s->begin_ptr[k + 1] - s->begin_ptr[k] - 1);
+                out_base[k] = tot;
+                nbb[0] = 0;
+                for (int b = 0; b < nb; ++b, ++q) {
+                        const int len = hkeep[q] ? bb[b + 1] - bb[b] : 0;
+                        if (len > 0) {
+                                gsrc.push_back(qoff[q]);
+                                gdst.push_back(tot + nbb[b]);
+                                glen.push_back(len);
+                        }
+                        nbb[b + 1] = nbb[b] + len;
+                }
+                tot += nbb[nb];
+        }
+        out_base[nnew] = tot;
+        const int64_t ng = (int64_t) glen.size();
+        if (ng > 0) {
+                T3NS_CUDA_TRY(cudaMemcpyAsync(tw.dev + S.goff_src, gsrc.data(), sizeof(int64_t) * ng,
+                                              cudaMemcpyHostToDevice, st));
+                T3NS_CUDA_TRY(cudaMemcpyAsync(tw.dev + S.goff_dst, gdst.data(), sizeof(int64_t) * ng,
+                                              cudaMemcpyHostToDevice, st));
+                T3NS_CUDA_TRY(cudaMemcpyAsync(tw.dev + S.glen, glen.data(), sizeof(int) * ng,
+                                              cudaMemcpyHostToDevice, st));
+                gather_blocks_kernel<<<(int) std::min<int64_t>(ng, 148 * 16), 256, 0, st>>>(
+                        ng, at<int64_t>(tw, S.goff_src), at<int64_t>(tw, S.goff_dst), at<int>(tw, S.glen),
+                        at<double>(tw, S.sum), at<double>(tw, S.out));
+                T3NS_CUDA_TRY(cudaGetLastError());
+                T3NS_CUDA_TRY(cudaMemcpyAsync(new_tel, tw.dev + S.out, sizeof(double) * tot,
+                                              cudaMemcpyDeviceToHost, st));
+        }
+        // the host vectors above are read by the copies: finish before they go
+        T3NS_CUDA_TRY(cudaStreamSynchronize(st));
+        return T3NS_OK;
 }
 
 }  // namespace
@@ -288,9 +485,19 @@ int pupdate_run(const t3ns_pupdate_desc *d, const double *t_tel, const double *o
         return finish_call(tw, o_NEW, new_tel, new_bytes);
 }
 
-int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst)
+// With sum (not null) the copies are unique operators that are summed into
+// the new set on the device (sum_run): dst, new_begin and out_base then
+// receive its kept blocks.
+int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst,
+                  const t3ns_sumunique_desc *sum = nullptr, int *new_begin = nullptr,
+                  int64_t *out_base = nullptr)
 {
         if (!d || !dst || d->nentries < 0) return set_error(T3NS_E_ARG, "scalecopy: bad descriptor");
+        int64_t nbl = 0;
+        if (sum) {
+                T3NS_TRY(check_sum_desc(sum, d->dst_elems, &nbl));
+                if (!new_begin || !out_base) return set_error(T3NS_E_ARG, "scalecopy: null output");
+        }
         for (int e = 0; e < d->nentries; ++e)
                 if (d->len[e] < 0 || d->src_off[e] < 0 || d->src_off[e] + d->len[e] > d->src_elems ||
                     d->dst_off[e] < 0 || d->dst_off[e] + d->len[e] > d->dst_elems)
@@ -301,11 +508,16 @@ int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst)
         const size_t o_len = L.input(d->len, d->nentries);
         const size_t o_scale = L.input(d->scale, d->nentries);
         const size_t o_S = L.input(src, d->src_elems);
+        SumLayout S{};
+        if (sum) sum_inputs(L, S, sum);
         const size_t in_end = L.c.off;
         const size_t o_D = L.c.take<double>(d->dst_elems);
+        const size_t zero_end = L.c.off;
+        if (sum) sum_work(L, S, sum, nbl);
         const size_t dst_bytes = sizeof(double) * d->dst_elems;
         ThreadWork &tw = thread_work();
-        T3NS_TRY(stage_call(tw, L, in_end, o_D, L.c.off, dst_bytes));
+        T3NS_TRY(stage_call(tw, L, in_end, o_D, zero_end,
+                            std::max(dst_bytes, sizeof(int) * (size_t) nbl)));
         if (d->nentries > 0) {
                 scalecopy_kernel<<<std::min(d->nentries, 148 * 16), 256, 0, tw.st>>>(
                         d->nentries, at<int64_t>(tw, o_dst_off), at<int64_t>(tw, o_src_off),
@@ -313,14 +525,39 @@ int scalecopy_run(const t3ns_scalecopy_desc *d, const double *src, double *dst)
                         at<double>(tw, o_D));
                 T3NS_CUDA_TRY(cudaGetLastError());
         }
+        if (sum) return sum_run(tw, S, sum, nbl, at<double>(tw, o_D), dst, new_begin, out_base);
         return finish_call(tw, o_D, dst, dst_bytes);
 }
 
+int sum_unique_run(const t3ns_sumunique_desc *sum, const double *unique_tel, double *new_tel,
+                   int *new_begin, int64_t *out_base)
+{
+        if (!sum || !new_tel || !new_begin || !out_base || sum->unique_elems < 0)
+                return set_error(T3NS_E_ARG, "sum_unique: bad arguments");
+        int64_t nbl = 0;
+        T3NS_TRY(check_sum_desc(sum, sum->unique_elems, &nbl));
+        CallLayout L;
+        const size_t o_U = L.input(unique_tel, sum->unique_elems);
+        SumLayout S{};
+        sum_inputs(L, S, sum);
+        const size_t in_end = L.c.off;
+        sum_work(L, S, sum, nbl);
+        ThreadWork &tw = thread_work();
+        T3NS_TRY(stage_call(tw, L, in_end, 0, 0, sizeof(int) * (size_t) nbl));
+        return sum_run(tw, S, sum, nbl, at<double>(tw, o_U), new_tel, new_begin, out_base);
+}
+
 int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o1_tel,
-                const double *o2_tel, double *new_tel)
+                const double *o2_tel, double *new_tel, const t3ns_sumunique_desc *sum = nullptr,
+                int *new_begin = nullptr, int64_t *out_base = nullptr)
 {
         if (!d || !new_tel || d->nunits < 0 || d->nentries < 0)
                 return set_error(T3NS_E_ARG, "bupdate: bad descriptor");
+        int64_t nbl = 0;
+        if (sum) {
+                T3NS_TRY(check_sum_desc(sum, d->new_elems, &nbl));
+                if (!new_begin || !out_base) return set_error(T3NS_E_ARG, "bupdate: null output");
+        }
         const int a = d->ax[0], b = d->ax[1], g = d->ax[2];
         if (a < 0 || a > 2 || b < 0 || b > 2 || g < 0 || g > 2 || a == b || a == g || b == g)
                 return set_error(T3NS_E_ARG, "bupdate: axes are not a permutation");
@@ -371,14 +608,18 @@ int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o
         const size_t o_T = L.input(t_tel, d->t_elems);
         const size_t o_O1 = L.input(o1_tel, d->o1_elems);
         const size_t o_O2 = L.input(o2_tel, d->o2_elems);
+        SumLayout S{};
+        if (sum) sum_inputs(L, S, sum);
         const size_t in_end = L.c.off;
         const size_t o_NEW = L.c.take<double>(d->new_elems);
         const size_t o_counter = L.c.take<int>(1);
         const size_t zero_end = L.c.off;
         const size_t o_scratch = L.c.take<double>((size_t) grid * (w1cap + w2cap));
+        if (sum) sum_work(L, S, sum, nbl);
         const size_t new_bytes = sizeof(double) * d->new_elems;
         ThreadWork &tw = thread_work();
-        T3NS_TRY(stage_call(tw, L, in_end, o_NEW, zero_end, new_bytes));
+        T3NS_TRY(stage_call(tw, L, in_end, o_NEW, zero_end,
+                            std::max(new_bytes, sizeof(int) * (size_t) nbl)));
         if (d->nunits > 0) {
                 bupdate_kernel<<<grid, kUpdThreads, 0, tw.st>>>(
                         make_int3(a, b, g), d->nunits, at<int>(tw, o_unit), at<int>(tw, o_dims),
@@ -389,6 +630,7 @@ int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o
                         w2cap, at<int>(tw, o_counter));
                 T3NS_CUDA_TRY(cudaGetLastError());
         }
+        if (sum) return sum_run(tw, S, sum, nbl, at<double>(tw, o_NEW), new_tel, new_begin, out_base);
         return finish_call(tw, o_NEW, new_tel, new_bytes);
 }
 
@@ -403,6 +645,28 @@ extern "C" int t3ns_bupdate_host(const t3ns_bupdate_desc *d, const double *t_tel
 extern "C" int t3ns_scalecopy_host(const t3ns_scalecopy_desc *d, const double *src, double *dst)
 {
         return t3ns::scalecopy_run(d, src, dst);
+}
+
+extern "C" int t3ns_sum_unique_host(const t3ns_sumunique_desc *s, const double *unique_tel,
+                                    double *new_tel, int *new_begin, int64_t *out_base)
+{
+        return t3ns::sum_unique_run(s, unique_tel, new_tel, new_begin, out_base);
+}
+
+extern "C" int t3ns_scalecopy_sum_host(const t3ns_scalecopy_desc *d, const t3ns_sumunique_desc *s,
+                                       const double *src, double *new_tel, int *new_begin,
+                                       int64_t *out_base)
+{
+        if (!s) return t3ns::set_error(T3NS_E_ARG, "scalecopy_sum: null sum descriptor");
+        return t3ns::scalecopy_run(d, src, new_tel, s, new_begin, out_base);
+}
+
+extern "C" int t3ns_bupdate_sum_host(const t3ns_bupdate_desc *d, const t3ns_sumunique_desc *s,
+                                     const double *t_tel, const double *o1_tel, const double *o2_tel,
+                                     double *new_tel, int *new_begin, int64_t *out_base)
+{
+        if (!s) return t3ns::set_error(T3NS_E_ARG, "bupdate_sum: null sum descriptor");
+        return t3ns::bupdate_run(d, t_tel, o1_tel, o2_tel, new_tel, s, new_begin, out_base);
 }
 
 extern "C" int t3ns_pupdate_host(const t3ns_pupdate_desc *d, const double *t_tel,

@@ -160,3 +160,23 @@ def sum_unique(rec, sch, unique):
             acc += sch["bu.instr_pref"][i] * unique[int(ubase[u]):int(ubase[u + 1])]
         out.append((begins[u0], acc))
     return out
+
+
+def compare_summed(rec, idx, got):
+    """Compares a new set after the sum and zero-block removal -- a list of
+    (begin array, elements) per operator -- with the reference's operator set
+    `idx` of the capture: identical surviving blocks, elements relative to
+    the largest reference element.  Returns that largest relative
+    difference."""
+    begins, ref = ops_structure(rec, idx)
+    assert len(begins) == len(got)
+    scale = max(np.abs(ref).max() if ref.size else 0.0, 1e-300)
+    worst, roff = 0.0, 0
+    for k, bb in enumerate(begins):
+        gbb, gel = got[k]
+        assert np.array_equal(np.asarray(gbb, np.int64), bb), k
+        rseg = ref[roff:roff + int(bb[-1])]
+        roff += int(bb[-1])
+        if rseg.size:
+            worst = max(worst, float(np.abs(gel - rseg).max()) / scale)
+    return worst

@@ -145,3 +145,25 @@ def test_dropin_preconditioner_matches_restated_reference(tmp_path):
     got = np.fromfile(fout, np.float64)
     want = precond_oracle.precondition(r, theta, dg, t)
     assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["hub10", "qc12"])
+def test_dropin_append_matches_reference_every_call(case, tmp_path):
+    """The drop-in's rOperators_append_phys (GPU scaled copies, device sum of
+    the unique operators, zero-block removal) against the reference's on
+    every call of a sweep: the reference harness runs both on the same input
+    in one process (--check-dropin) and compares the new sets -- the same
+    operators, sectors and surviving blocks, the elements to 1e-12 of the
+    largest (reference src/rOperators_pUpdate.c:665-673)."""
+    need(RUN_REF, DROPIN)
+    if case == "hub10":
+        args = HUB10 + ["--regime", "128,128,0,2,1e-5,100,1,1e-8,0"]
+    else:
+        fc = synthetic_qc_fcidump(tmp_path / "qc12.FCIDUMP", 12, 12, 0, 72)
+        args = ["--net", os.path.join(NET, "t3ns_12.netw"), "--inter", fc, "--symm",
+                "Z2,U1,SU2", "--ts", "0,12,0", "--regime", "64,64,0,2,1e-5,100,1,1e-8,0"]
+    out = run(RUN_REF, args + ["--init", "c", "--check-dropin", DROPIN])
+    diffs = [float(v) for v in re.findall(r"CHECK_APPEND \d+ (\S+)", out)]
+    assert len(diffs) >= 10
+    assert all(0.0 <= v <= 1e-12 for v in diffs), max(diffs)

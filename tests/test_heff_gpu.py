@@ -243,3 +243,25 @@ def test_ordered_configs_switch_precision(torch_cuda):
     plan.set_precision(T3NS_PREC_FP64)
     assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= MATVEC_RTOL
     plan.close()
+
+
+@pytest.mark.parametrize("config", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("path", golden_steps(), ids=lambda p: p.split("/")[-1])
+def test_every_config_on_golden_steps(path, config, torch_cuda):
+    """Every configuration in both precisions on every golden step (both
+    DMRG-type two-operator steps and T3NS steps), with the device status
+    read after each matvec."""
+    import ctypes as C
+    from t3ns_b200.native import T3NS_PREC_3XTF32
+    torch = torch_cuda
+    s = read_step(path)
+    st = torch.cuda.current_stream().cuda_stream
+    for prec, tol in ((0, MATVEC_RTOL), (T3NS_PREC_3XTF32, SPLIT_RTOL)):
+        plan = HeffPlan(StepDesc(s), prec)
+        plan.set_config(config)
+        x = torch.from_numpy(s["x0"]).cuda()
+        y = torch.empty_like(x)
+        plan.matvec_device(x.data_ptr(), y.data_ptr(), st)
+        assert plan.lib.t3ns_heff_check_status(plan.h, C.c_void_p(st)) == 0
+        assert _rel(y.cpu().numpy(), s["y0"]) <= tol
+        plan.close()
