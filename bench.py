@@ -49,9 +49,18 @@ UNIT = "TFLOP/s"
 DEFAULT_WORKLOAD_DIR = os.path.join(ROOT, "oracle", "_ref", "workloads")
 
 
+# the headline step: the 24-orbital QC Hamiltonian at D=512, SITE_SIZE 2
+DEFAULT_WORKLOAD = "qc24_D512_step005.t3c"
+# the microbenchmark steps: three-site D=1024 steps of the same Hamiltonian
+MICRO_PATTERN = "qc24_D1024_s3_step*.t3c"
+
+
 def pick_workload(path: str | None) -> str:
     if path:
         return path
+    p = os.path.join(DEFAULT_WORKLOAD_DIR, DEFAULT_WORKLOAD)
+    if os.path.exists(p):
+        return p
     cands = sorted(glob.glob(os.path.join(DEFAULT_WORKLOAD_DIR, "*.t3c")),
                    key=os.path.getsize)
     if not cands:
@@ -325,13 +334,42 @@ def sweep_comparison(timeout=900):
                                env=env, timeout=timeout)
             if r.returncode != 0:
                 return {"error": f"{name} {prec}: exit {r.returncode}"}
-            e = float(re.findall(r"FINAL_ENERGY (\S+)", r.stdout)[-1])
-            t = float(re.findall(r"SWEEP_SECONDS (\S+)", r.stdout)[-1])
-            rec[prec] = {"sweep_seconds": t, "energy": e}
-        rec["speedup_mixed_vs_fp64"] = rec["fp64"]["sweep_seconds"] / rec["3xtf32"]["sweep_seconds"]
-        rec["abs_dE_mixed_vs_fp64"] = abs(rec["3xtf32"]["energy"] - rec["fp64"]["energy"])
+            rec[prec] = parse_sweep_run(r.stdout)
+        f, m = rec["fp64"], rec["3xtf32"]
+        rec["speedup_mixed_vs_fp64"] = f["sweep_seconds"] / m["sweep_seconds"]
+        rec["matvec_bucket_speedup_mixed_vs_fp64"] = (
+            f["timers"].get("Heff T3NS: matvec", 0) + f["timers"].get("Heff DMRG: matvec", 0)) / max(
+            m["timers"].get("Heff T3NS: matvec", 0) + m["timers"].get("Heff DMRG: matvec", 0), 1e-12)
+        rec["abs_dE_mixed_vs_fp64"] = abs(m["energy"] - f["energy"])
         out[name] = rec
+    out["note"] = ("timers are the reference's own buckets over the whole scheme "
+                   "(src/optimize_network.c:43-95): 'Heff ...: matvec' is the Davidson solves, "
+                   "'prepare data' holds the plan build and the autotuner, so the matvec bucket "
+                   "is the mixed-vs-FP64 comparison; davidson_iterations counts matvecs, "
+                   "fp64_iterations those in FP64")
     return out
+
+
+_TIMER = re.compile(r"^ \* (.+?)\s+:: ([0-9.]+) sec", re.M)
+
+
+def parse_sweep_run(stdout: str) -> dict:
+    """Final energy, sweep seconds, sweeps executed, the reference's timers
+    for the whole optimisation scheme, and the Davidson iteration counts
+    (all and FP64) of one run of the drop-in driver."""
+    tail = stdout.split("TIMERS FOR OPTIMIZATION SCHEME")[-1]
+    timers = {k.strip(): float(v) for k, v in _TIMER.findall(tail)}
+    return {
+        "sweep_seconds": float(re.findall(r"SWEEP_SECONDS (\S+)", stdout)[-1]),
+        "energy": float(re.findall(r"FINAL_ENERGY (\S+)", stdout)[-1]),
+        "sweeps": sum(int(k) for k in re.findall(r"END OF REGIME \d+ AFTER (\d+)/\d+ SWEEPS", stdout)),
+        "timers": timers,
+        "timers_total_vs_sweep_seconds": timers.get("Total time", 0.0) /
+        max(float(re.findall(r"SWEEP_SECONDS (\S+)", stdout)[-1]), 1e-12),
+        "davidson_solves": len(re.findall(r"Davidson: \(iter: ", stdout)),
+        "davidson_iterations": sum(int(x) for x in re.findall(r"Davidson: \(iter: (\d+)\)", stdout)),
+        "fp64_iterations": sum(int(x) for x in re.findall(r"\(fp64 iter: (\d+)\)", stdout)),
+    }
 
 
 def davidson_comparison(path=None, max_its=100, seed=7):
@@ -490,6 +528,85 @@ def serving_stream():
     return summary
 
 
+def microbench_d1024(args, peak, reps=None):
+    """The batched matvec microbenchmark: the three-site D=1024 steps of the
+    24-orbital Hamiltonian (structure from the reference sweep, operator
+    values from a fixed seed).  Per step: block statistics, F, the grouped
+    persistent FP64 launch (autotuned), the same kernel dispatched block by
+    block, and the split-precision (3xTF32) matvec with its error against
+    FP64; CUDA events, L2 flushed between iterations."""
+    import torch
+
+    from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_FP64, HeffPlan, StepDesc
+    from t3ns_b200.stepfile import read_step
+    files = sorted(glob.glob(os.path.join(DEFAULT_WORKLOAD_DIR, MICRO_PATTERN)))
+    if not files:
+        return None
+    reps = reps or max(3, min(args.steps, 5))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in ts]))
+
+    out = []
+    for f in files:
+        s = read_step(f)
+        sizes = np.diff(s["beginblock"].astype(np.int64))
+        plan = HeffPlan(StepDesc(s))
+        F = plan.stats["flops_ref"]
+        g = torch.Generator(device="cpu").manual_seed(5)
+        x = torch.randn(plan.size, generator=g, dtype=torch.float64)
+        x = (x / x.norm()).cuda()
+        y = torch.empty_like(x)
+        sh = stream.cuda_stream
+        tune = plan.autotune(reps=1)
+        t64 = timed(lambda: plan.matvec_device(x.data_ptr(), y.data_ptr(), sh))
+        cfg64 = plan.config()
+        y64 = y.clone()
+        tblk = timed(lambda: plan.matvec_device_per_block(x.data_ptr(), y.data_ptr(), sh))
+        nblk = plan.last_launches()
+        plan.set_precision(T3NS_PREC_3XTF32)
+        stune = plan.autotune(reps=1)
+        tsp = timed(lambda: plan.matvec_device(x.data_ptr(), y.data_ptr(), sh))
+        err = float((y - y64).norm() / y64.norm())
+        cfgsp = plan.config()
+        plan.set_precision(T3NS_PREC_FP64)
+        plan.close()
+        out.append({
+            "step": os.path.basename(f), "blocks": int(s["nrblocks"][0]), "psi_elems": int(sizes.sum()),
+            "block_size_quantiles": {q: int(np.quantile(sizes, q)) for q in (0.5, 0.9, 1.0)},
+            "merge_instr": int(s["iset.nr_instr"][0]), "flops_per_matvec": F,
+            "fp64_grouped": {"ms": t64, "tflops": F / t64 / 1e9, "kernel_config": cfg64,
+                             "autotune_ms": tune,
+                             "roofline_frac": (F / t64 / 1e9) / peak if peak else None},
+            "fp64_per_block_dispatch": {"ms": tblk, "tflops": F / tblk / 1e9, "launches": nblk},
+            "grouped_speedup_vs_per_block": tblk / t64,
+            "split_3xtf32": {"ms": tsp, "tflops": F / tsp / 1e9, "kernel_config": cfgsp,
+                             "autotune_ms": stune, "speedup_vs_fp64": t64 / tsp,
+                             "rel_err_vs_fp64": err},
+            "bf16x3": "not built",
+        })
+        del x, y, y64
+        torch.cuda.empty_cache()
+    return {"steps": out, "l2": "flushed between iterations",
+            "data": "block structure and schedule from the reference's three-site D=1024 sweep of "
+                    "the synthetic 24-orbital Hamiltonian; operator values from a fixed seed"}
+
+
 def traffic_from_profile(workload_path, kernel_config):
     """DRAM bytes (read + write) of one FP64 heff_kernel launch in kernel
     configuration `kernel_config` on this workload, from the ncu capture
@@ -552,6 +669,8 @@ def main():
                     help="skip the whole-sweep FP64 vs split-precision comparison")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the request-stream (serving) measurement")
+    ap.add_argument("--no-micro", action="store_true",
+                    help="skip the three-site D=1024 matvec microbenchmark")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -605,8 +724,10 @@ def main():
     if world > 1:
         # the CPU baseline, Davidson, sweep, serving and update figures are
         # single-GPU measurements, taken at N=1 only
-        args.no_cpu_baseline = args.no_sweep = args.no_serving = True
+        args.no_cpu_baseline = args.no_sweep = args.no_serving = args.no_micro = True
     if rank == 0:
+        if not args.no_micro:
+            out["microbench_D1024"] = microbench_d1024(args, out["roofline"]["peak"])
         if not args.no_cpu_baseline:
             cb = cpu_baseline(pick_workload(args.workload), samples=1)
             if cb:

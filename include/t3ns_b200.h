@@ -106,6 +106,14 @@ int t3ns_heff_create(const t3ns_heff_desc *desc, int precision, t3ns_heff **out)
  * Replaces exec_secondrun (reference src/Heff.c:945-1000). */
 int t3ns_heff_matvec_device(t3ns_heff *h, const double *x, double *y, void *stream);
 
+/* The same product dispatched block by block: one launch of the matvec
+ * kernel per output block, over that block's work units (FP64; the grouped
+ * single launch above is the engine's path).  For measuring what one
+ * persistent grouped launch saves over per-block dispatch, the way the
+ * reference's loop over new blocks in exec_secondrun (src/Heff.c:945-1000)
+ * would map to the GPU. */
+int t3ns_heff_matvec_device_per_block(t3ns_heff *h, const double *x, double *y, void *stream);
+
 /* Same with host buffers: x is copied to the device, y back to the host.
  * Synchronises and returns T3NS_E_DEVICE if the kernel reported an error. */
 int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y);

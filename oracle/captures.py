@@ -98,12 +98,13 @@ def trim(path, out=None):
     write_step(out or path, s)
 
 
-def structure_only(path, out):
+def structure_only(path, out, compress=False):
     """Writes the step's structure without operator values or vectors: each
     ops{i}.tel record becomes ops{i}.tel_len, and the loaders fill the
     operator elements from a fixed seed (the matvec's cost and schedule depend
     only on the structure).  Used for benchmark workloads too large to ship
-    with their values."""
+    with their values; compress: arrays above 1 MiB zlib-compressed (Python
+    readers only)."""
     s = read_step(path)
     rec = {}
     for k, v in s.items():
@@ -113,7 +114,7 @@ def structure_only(path, out):
             rec[k + "_len"] = np.array([v.size], np.int64)
             continue
         rec[k] = v
-    write_step(out, rec)
+    write_step(out, rec, compress_above=(1 << 20) if compress else None)
 
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -226,8 +227,8 @@ if __name__ == "__main__":
     if sys.argv[1] == "d512":
         ensure_d512()
         sys.exit(0)
-    if sys.argv[1] == "structure":
-        structure_only(sys.argv[2], sys.argv[3])
+    if sys.argv[1] in ("structure", "structure-z"):
+        structure_only(sys.argv[2], sys.argv[3], compress=sys.argv[1] == "structure-z")
         print(sys.argv[3], os.path.getsize(sys.argv[3]) >> 20, "MiB")
     else:
         for p in sys.argv[1:]:

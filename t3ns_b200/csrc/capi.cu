@@ -119,6 +119,13 @@ static int upload_tiles(t3ns_heff *h, int cfg)
         T3NS_TRY(upload(h, &dt.pairs, tp.pairs.data(), tp.pairs.size()));
         T3NS_TRY(upload(h, &dt.units, tp.units.data(), tp.units.size()));
         dt.n_units = (int) tp.units.size();
+        dt.block_runs.clear();
+        for (int u = 0; u < dt.n_units; ++u)
+                if (u == 0 || tp.units[u].nb != tp.units[u - 1].nb) {
+                        if (u) dt.block_runs.push_back(u);
+                        dt.block_runs.push_back(u);
+                }
+        if (dt.n_units) dt.block_runs.push_back(dt.n_units);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
         dt.grid = std::max(1, std::min(dt.n_units, kCfgs[cfg].ctas_per_sm * sms));
@@ -236,6 +243,12 @@ int t3ns_heff_matvec_device(t3ns_heff *h, const double *x, double *y, void *stre
 {
         if (!h || !x || !y) return set_error(T3NS_E_ARG, "null argument");
         return launch_heff(h->dp, h->precision, x, y, (cudaStream_t) stream, &h->last_launches);
+}
+
+int t3ns_heff_matvec_device_per_block(t3ns_heff *h, const double *x, double *y, void *stream)
+{
+        if (!h || !x || !y) return set_error(T3NS_E_ARG, "null argument");
+        return launch_heff(h->dp, h->precision, x, y, (cudaStream_t) stream, &h->last_launches, true);
 }
 
 int t3ns_heff_matvec_host(t3ns_heff *h, const double *x, double *y)

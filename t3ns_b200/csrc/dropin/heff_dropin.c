@@ -647,8 +647,9 @@ int davidson(double *result, double *energy, int size, int max_vecs, int keep_de
                 return -1;
         }
         if (rc < 0) die("davidson");
-        printf("   * Davidson: (iter: %d), (d_eig: %.1e), (trunc: %.1e), (time: %.3g sec)\n",
-               info.iterations, info.d_energy, info.residual, info.seconds);
+        printf("   * Davidson: (iter: %d), (d_eig: %.1e), (trunc: %.1e), (time: %.3g sec), "
+               "(fp64 iter: %d)\n",
+               info.iterations, info.d_energy, info.residual, info.seconds, info.fp64_iterations);
         if (info.residual > davidson_tol) printf("     - Davidson stopped before converging.\n");
         return rc;
 }

@@ -1671,8 +1671,37 @@ int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s)
 }
 
 int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
-                int *launches)
+                int *launches, bool per_block)
 {
+        if (per_block) {
+                // the same kernel, one launch per output block (its own unit run)
+                const DeviceTiles &full = dp.tiles[dp.active];
+                if (!full.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
+                if (precision != T3NS_PREC_FP64)
+                        return set_error(T3NS_E_ARG, "matvec: per-block dispatch is FP64 only");
+                T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
+                DevicePlan one = dp;
+                int n = 0;
+                for (size_t r = 0; r + 1 < full.block_runs.size(); r += 2) {
+                        DeviceTiles &dt = one.tiles[dp.active];
+                        dt.units = full.units + full.block_runs[r];
+                        dt.n_units = full.block_runs[r + 1] - full.block_runs[r];
+                        dt.grid = std::max(1, std::min(dt.n_units, full.grid));
+                        T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
+                        int rc;
+                        switch (dp.active) {
+                        case 0: rc = launch_cfg<CfgLarge, double>(one, dt, x, dp.ops, y, s); break;
+                        case 1: rc = launch_cfg<CfgSmall, double>(one, dt, x, dp.ops, y, s); break;
+                        case 2: rc = launch_cfg<CfgWide, double>(one, dt, x, dp.ops, y, s); break;
+                        case 3: rc = launch_v2<CfgV2Wide, false>(one, dt, x, y, s); break;
+                        default: rc = launch_v2<CfgV2Large, false>(one, dt, x, y, s); break;
+                        }
+                        T3NS_TRY(rc);
+                        ++n;
+                }
+                if (launches) *launches = n;
+                return T3NS_OK;
+        }
         const DeviceTiles &dt = dp.tiles[dp.active];
         if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
         const bool split = precision == T3NS_PREC_3XTF32;

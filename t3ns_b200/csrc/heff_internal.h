@@ -106,6 +106,9 @@ struct DeviceTiles {
         HeffUnit *units = nullptr;
         int n_units = 0;
         int grid = 0;
+        // runs [block_runs[2i], block_runs[2i+1]) of the units of one output
+        // block (the unit list keeps a block's tiles together)
+        std::vector<int> block_runs;
 };
 
 struct DevicePlan {
@@ -139,8 +142,11 @@ int tile_plan(HostPlan &hp, int cfg);
 int launch_heff_fp64(const DevicePlan &dp, const double *x, double *y, cudaStream_t s,
                      int *launches);
 // The matvec in precision T3NS_PREC_FP64 or T3NS_PREC_3XTF32 (FP64 in and out).
+// per_block: one launch per output block over that block's units (the
+// per-block dispatch a loop over blocks would issue), for comparison with the
+// single persistent launch.
 int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
-                int *launches);
+                int *launches, bool per_block = false);
 int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s);
 // {hi, lo} pairs of the transposed operators.
 int convert_to_pairs(const double *a, float2 *b, int64_t n, cudaStream_t s);

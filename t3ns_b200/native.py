@@ -85,6 +85,8 @@ def load(path: str | None = None):
     lib = C.CDLL(p)
     lib.t3ns_heff_create.argtypes = [C.POINTER(HeffDesc), C.c_int, C.POINTER(C.c_void_p)]
     lib.t3ns_heff_matvec_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.t3ns_heff_matvec_device_per_block.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
+                                                      C.c_void_p]
     lib.t3ns_heff_matvec_host.argtypes = [C.c_void_p, _f64p, _f64p]
     lib.t3ns_heff_diagonal_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.t3ns_heff_diagonal_host.argtypes = [C.c_void_p, _f64p]
@@ -260,6 +262,12 @@ class HeffPlan:
     def matvec_device(self, x_ptr: int, y_ptr: int, stream: int = 0):
         check(self.lib.t3ns_heff_matvec_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
                                                C.c_void_p(stream)), "matvec_device")
+
+    def matvec_device_per_block(self, x_ptr: int, y_ptr: int, stream: int = 0):
+        """The same product with one kernel launch per output block."""
+        check(self.lib.t3ns_heff_matvec_device_per_block(self.h, C.c_void_p(x_ptr),
+                                                         C.c_void_p(y_ptr), C.c_void_p(stream)),
+              "matvec_device_per_block")
 
     def diagonal_host(self) -> np.ndarray:
         d = np.empty(self.size)

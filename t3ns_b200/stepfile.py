@@ -11,9 +11,14 @@ matvec / diagonal / Davidson outputs.
 
 Layout: the 8-byte magic ``T3NSCAP1`` followed by records
 ``{char name[48]; int32 dtype; int32 pad; int64 count; payload}`` with dtype
-1 = int32, 2 = int64, 3 = float64, little endian.
+1 = int32, 2 = int64, 3 = float64, little endian.  A dtype with bit 0x10 set
+marks a zlib-compressed payload: an int64 byte length, then the compressed
+bytes of the ``count`` elements (used for the large schedule arrays of
+structure-only benchmark files).
 """
 from __future__ import annotations
+
+import zlib
 
 import numpy as np
 
@@ -40,10 +45,17 @@ def read_step(path) -> dict:
     while pos < len(buf):
         hdr = np.frombuffer(buf, _HDR, 1, pos)[0]
         pos += _HDR.itemsize
-        dt = np.dtype(_DTYPES[int(hdr["dtype"])])
+        code = int(hdr["dtype"])
+        dt = np.dtype(_DTYPES[code & 0xF])
         n = int(hdr["count"])
-        arr = np.frombuffer(buf, dt, n, pos).copy()
-        pos += n * dt.itemsize
+        if code & 0x10:
+            nb = int(np.frombuffer(buf, np.int64, 1, pos)[0])
+            pos += 8
+            arr = np.frombuffer(zlib.decompress(buf[pos:pos + nb]), dt, n).copy()
+            pos += nb
+        else:
+            arr = np.frombuffer(buf, dt, n, pos).copy()
+            pos += n * dt.itemsize
         out[hdr["name"].decode()] = arr
     for i in range(3):
         if f"ops{i}.tel_len" in out and f"ops{i}.tel" not in out:
@@ -51,8 +63,10 @@ def read_step(path) -> dict:
     return out
 
 
-def write_step(path, rec: dict) -> None:
-    """Write ``{name: ndarray}`` in the step-file layout (int32/int64/float64)."""
+def write_step(path, rec: dict, compress_above: int | None = None) -> None:
+    """Write ``{name: ndarray}`` in the step-file layout (int32/int64/float64);
+    arrays of more than ``compress_above`` bytes are written zlib-compressed
+    (never, by default)."""
     codes = {np.dtype(np.int32): 1, np.dtype(np.int64): 2, np.dtype(np.float64): 3}
     with open(path, "wb") as f:
         f.write(b"T3NSCAP1")
@@ -60,7 +74,14 @@ def write_step(path, rec: dict) -> None:
             arr = np.ascontiguousarray(arr)
             h = np.zeros(1, _HDR)
             h["name"] = name.encode()
-            h["dtype"] = codes[arr.dtype]
             h["count"] = arr.size
-            f.write(h.tobytes())
-            f.write(arr.tobytes())
+            if compress_above is not None and arr.nbytes > compress_above:
+                payload = zlib.compress(arr.tobytes(), 6)
+                h["dtype"] = codes[arr.dtype] | 0x10
+                f.write(h.tobytes())
+                f.write(np.array([len(payload)], np.int64).tobytes())
+                f.write(payload)
+            else:
+                h["dtype"] = codes[arr.dtype]
+                f.write(h.tobytes())
+                f.write(arr.tobytes())

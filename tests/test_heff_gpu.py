@@ -265,3 +265,25 @@ def test_every_config_on_golden_steps(path, config, torch_cuda):
         assert plan.lib.t3ns_heff_check_status(plan.h, C.c_void_p(st)) == 0
         assert _rel(y.cpu().numpy(), s["y0"]) <= tol
         plan.close()
+
+
+@pytest.mark.parametrize("config", [0, 2, 3])
+@pytest.mark.parametrize("path", STEPS[::5], ids=lambda p: "/".join(p.split("/")[-2:]))
+def test_per_block_dispatch_matches_grouped_launch(path, config, torch_cuda):
+    """One launch per output block (t3ns_heff_matvec_device_per_block) gives
+    the grouped single launch's product and the reference's, with one launch
+    per block that has work."""
+    torch = torch_cuda
+    s = read_step(path)
+    plan = HeffPlan(StepDesc(s))
+    plan.set_config(config)
+    x = torch.from_numpy(s["x0"]).cuda()
+    y1, y2 = torch.empty_like(x), torch.empty_like(x)
+    st = torch.cuda.current_stream().cuda_stream
+    plan.matvec_device(x.data_ptr(), y1.data_ptr(), st)
+    plan.matvec_device_per_block(x.data_ptr(), y2.data_ptr(), st)
+    torch.cuda.synchronize()
+    assert plan.last_launches() >= 1
+    assert _rel(y2.cpu().numpy(), y1.cpu().numpy()) <= 1e-14
+    assert _rel(y2.cpu().numpy(), s["y0"]) <= MATVEC_RTOL
+    plan.close()
