@@ -214,7 +214,38 @@ def ensure_d512(threads=None):
             structure_only(src, out)
 
 
+def ensure_d1024_s3(threads=None):
+    """The three-site microbenchmark steps: the 24-orbital synthetic QC
+    Hamiltonian at D=1024 with SITE_SIZE 3 (branching site plus two physical
+    sites, reference src/network.c:605-616), the first three steps of the
+    sweep whose site tensor has 4e6 to 1.8e7 elements (one reference matvec
+    each, to build the replay schedule; no Davidson).  The full captures
+    (several GB) stay in oracle/_ref/captures/qc24_D1024_s3; the benchmark
+    reads their compressed structure-only copies in oracle/_ref/workloads.
+    About an hour on 8 cores: the initial renormalised operators and one
+    reference matvec per step before the last capture dominate."""
+    threads = threads or os.cpu_count() or 1
+    d = os.path.join(REF, "captures", "qc24_D1024_s3")
+    if not any(f.startswith("step_") for f in (os.listdir(d) if os.path.isdir(d) else [])):
+        _capture(d, ["--net", os.path.join(NETS, "t3ns_24.netw"), "--inter", _fcidump(24),
+                     "--symm", "Z2,U1,SU2", "--ts", "0,24,0",
+                     "--regime", "1024,1024,0,3,1e-5,100,1,1e-8,0"],
+                 ["--capture-min", "4000000", "--capture-max", "18000000",
+                  "--capture-limit", "3", "--capture-stop", "--capture-noeig",
+                  "--capture-nvec", "1"], threads)
+    wl = os.path.join(REF, "workloads")
+    os.makedirs(wl, exist_ok=True)
+    for f in sorted(os.listdir(d)):
+        if f.startswith("step_") and f.endswith(".t3c"):
+            out = os.path.join(wl, "qc24_D1024_s3_" + f.replace("_", ""))
+            if not os.path.exists(out):
+                structure_only(os.path.join(d, f), out, compress=True)
+
+
 if __name__ == "__main__":
+    if sys.argv[1] == "d1024":
+        ensure_d1024_s3()
+        sys.exit(0)
     if sys.argv[1] == "small":
         ensure_small()
         sys.exit(0)

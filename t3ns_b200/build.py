@@ -45,12 +45,14 @@ def build_engine(force: bool = False) -> str:
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(INCLUDE, "t3ns_b200.h"))
     if force or _stale(out, deps):
-        objs = []
-        for s in srcs:
-            o = os.path.join(LIBDIR, os.path.basename(s) + ".o")
-            _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-                  "-Xptxas", "-warn-spills", "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o])
-            objs.append(o)
+        from concurrent.futures import ThreadPoolExecutor
+        objs = [os.path.join(LIBDIR, os.path.basename(s) + ".o") for s in srcs]
+        cmds = [[NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                 "-Xptxas", "-warn-spills", "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
+                for s, o in zip(srcs, objs)]
+        # the translation units compile independently (heff.cu dominates)
+        with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+            list(ex.map(_run, cmds))
         _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart_static", "-lrt", "-ldl",
               "-lpthread"])
     return out

@@ -319,7 +319,7 @@ __device__ __forceinline__ void grouped_stage_t(const int *w, int rows, int ldop
                                                 const double *__restrict__ ops, const double *in,
                                                 int in_gs, double *out, int out_gs,
                                                 const double *scale, double *scratch,
-                                                int scratch_cap)
+                                                int scratch_cap, const int *in_idx)
 {
         int M, N, K, ak, bk, bn, cn;
         RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
@@ -372,7 +372,7 @@ __device__ __forceinline__ void grouped_stage_t(const int *w, int rows, int ldop
                                                         rs, bk, bn, K, M, N, m0, n0, lr, lc);
                 } else {
                         const double *op = ops + opoff[g0];
-                        const double *tin = in + g0 * in_gs;
+                        const double *tin = in + (in_idx ? in_idx[g0] : g0) * in_gs;
                         if constexpr (AX == 0)
                                 warp_tile_mma<RM, RN, true>(d, op, ak, rs, tin, bk, bn, K, M, N, m0,
                                                             n0, lr, lc);
@@ -424,7 +424,7 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                                               const double *__restrict__ ops, const double *in,
                                               int in_gs, double *out, int out_gs,
                                               const double *scale, double *scratch = nullptr,
-                                              int scratch_cap = 0)
+                                              int scratch_cap = 0, const int *in_idx = nullptr)
 {
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
@@ -434,13 +434,13 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                 constexpr int AX = decltype(axc)::value;
                 if (M <= 8)
                         grouped_stage_t<ACC, 1, 4, NW, AX>(w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                           out_gs, scale, scratch, scratch_cap);
+                                                           out_gs, scale, scratch, scratch_cap, in_idx);
                 else if (N <= 8)
                         grouped_stage_t<ACC, 4, 1, NW, AX>(w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                           out_gs, scale, scratch, scratch_cap);
+                                                           out_gs, scale, scratch, scratch_cap, in_idx);
                 else
                         grouped_stage_t<ACC, 2, 2, NW, AX>(w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                           out_gs, scale, scratch, scratch_cap);
+                                                           out_gs, scale, scratch, scratch_cap, in_idx);
         };
         if (ax == 0) go(std::integral_constant<int, 0>{});
         else if (ax == 1) go(std::integral_constant<int, 1>{});
@@ -564,7 +564,8 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
                                                   const float2 *__restrict__ ops,
                                                   const float2 *in, int in_gs, OutT *out,
                                                   int out_gs, const float *scale, bool swap,
-                                                  float *scratch, int scratch_cap)
+                                                  float *scratch, int scratch_cap,
+                                                  const int *in_idx)
 {
         int M, N, K, ak, bk, bn, cn;
         RowSplit rs{1 << 30, 1.0f / (1 << 30), 0, 0};
@@ -615,7 +616,7 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
                                 for (int q = 0; q < 4; ++q) d[i][j][q] = 0.f;
                 for (int gg = g0; gg < g1; gg += gstep) {
                         const float2 *op = ops + opoff[gg];
-                        const float2 *tin = in + gg * in_gs;
+                        const float2 *tin = in + (!ACC && in_idx ? in_idx[gg] : gg) * in_gs;
                         const float2 *Ab = ax == 0 ? op : tin;
                         const float2 *Bb = ax == 0 ? tin : op;
                         if (swap)
@@ -670,7 +671,7 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                                               const int64_t *opoff, const float2 *__restrict__ ops,
                                               const float2 *in, int in_gs, OutT *out, int out_gs,
                                               const float *scale, float2 *scratch = nullptr,
-                                              int scratch_cap = 0)
+                                              int scratch_cap = 0, const int *in_idx = nullptr)
 {
         // the scratch holds FP32 partial tiles: two per float2 slot
         float *fs = reinterpret_cast<float *>(scratch);
@@ -684,13 +685,13 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
         const int Mt = swap ? N : M, Nt = swap ? M : N;
         if (Mt <= 16)
                 grouped_stage_x_t<ACC, 1, 4, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                 out_gs, scale, swap, fs, fcap);
+                                                 out_gs, scale, swap, fs, fcap, in_idx);
         else if (Nt <= 8)
                 grouped_stage_x_t<ACC, 2, 1, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                 out_gs, scale, swap, fs, fcap);
+                                                 out_gs, scale, swap, fs, fcap, in_idx);
         else
                 grouped_stage_x_t<ACC, 2, 2, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out,
-                                                 out_gs, scale, swap, fs, fcap);
+                                                 out_gs, scale, swap, fs, fcap, in_idx);
 }
 
 // Element types of the kernel: operand storage T, the output tile's
@@ -724,7 +725,8 @@ constexpr size_t smem_bytes_t()
 {
         return sizeof(typename Elem<T>::Acc) * Caps<Cfg, T>::kOut +
                sizeof(T) * (Caps<Cfg, T>::kPsi + Caps<Cfg, T>::kW) +
-               sizeof(typename Elem<T>::Scale) * kGMax + sizeof(int64_t) * 3 * kGMax + 64;
+               sizeof(typename Elem<T>::Scale) * kGMax + sizeof(int64_t) * 4 * kGMax +
+               sizeof(int) * kGMax + 64;
 }
 
 template <class Cfg, class T>
@@ -745,7 +747,9 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
         T *W = PSI + C::kPsi;
         Scale *PREF = reinterpret_cast<Scale *>(W + C::kW);
         int64_t *OPOFF = reinterpret_cast<int64_t *>(PREF + kGMax);   // [3][kGMax]
-        int *UNIT = reinterpret_cast<int *>(OPOFF + 3 * kGMax);
+        int64_t *UOFF = OPOFF + 3 * kGMax;     // distinct first-stage operators of a group
+        int *AIDX = reinterpret_cast<int *>(UOFF + kGMax);   // term -> its first-stage result
+        int *UNIT = AIDX + kGMax;              // [0] unit, [1] group size, [2] distinct count
         const int tid = threadIdx.x;
 
         for (;;) {
@@ -789,36 +793,80 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                                 in0 = PSI;
                         }
                         const int G = min(kGMax, C::kW / (s1 + s2));
-                        T *W1 = W, *W2 = W + G * s1;
+                        T *W1 = W;
                         const int nterm = pr.t1 - pr.t0;
-                        for (int t0 = 0; t0 < nterm; t0 += G) {
-                                const int g = min(G, nterm - t0);
-                                if (tid < g) {
+                        for (int t0 = 0, g = 0; t0 < nterm; t0 += g) {
+                                const int cand = min(nst == 3 ? kGMax : G, nterm - t0);
+                                if (tid < cand) {
                                         const HeffTask &tk = tasks[pr.t0 + t0 + tid];
                                         for (int s = 0; s < 3; ++s)
                                                 OPOFF[s * kGMax + tid] = tk.op_off[ax[s]] + row0[ax[s]];
                                         PREF[tid] = (Scale) tk.pref;
                                 }
                                 __syncthreads();
-                                // the first stage reads the staged block (shared memory) or
-                                // the block in global memory: one call site for each, so each
-                                // is compiled for its own address space
                                 if (nst == 3) {
+                                        // Terms that apply the same first-stage operator share
+                                        // its result (the host sorts a pair's terms so they sit
+                                        // next to each other): warp 0 numbers the runs of equal
+                                        // first-stage operators and takes the longest prefix of
+                                        // the candidates whose n1 first-stage results and g
+                                        // second-stage results fit the intermediate buffer.
+                                        if (tid < 32) {
+                                                int base = 0, gsel = 0, n1 = 0;
+                                                for (int h = 0; h < kGMax / 32; ++h) {
+                                                        const int t = tid + 32 * h;
+                                                        const bool in = t < cand;
+                                                        const bool first = in && (t == 0 || OPOFF[t] != OPOFF[t - 1]);
+                                                        const unsigned fb = __ballot_sync(0xffffffffu, first);
+                                                        const int incl = base + __popc(fb & (0xffffffffu >> (31 - tid)));
+                                                        const bool fits = in && (int64_t) incl * s1 +
+                                                                                (int64_t) (t + 1) * s2 <= C::kW;
+                                                        const unsigned ok = __ballot_sync(0xffffffffu, fits);
+                                                        if (in) AIDX[t] = incl - 1;
+                                                        if (first) UOFF[incl - 1] = OPOFF[t];
+                                                        if (ok) {
+                                                                const int last = 31 - __clz(ok);
+                                                                gsel = 32 * h + last + 1;
+                                                                n1 = __shfl_sync(0xffffffffu, incl, last);
+                                                        }
+                                                        base += __popc(fb);
+                                                }
+                                                if (tid == 0) {
+                                                        UNIT[1] = gsel;
+                                                        UNIT[2] = n1;
+                                                }
+                                        }
+                                        __syncthreads();
+                                        g = UNIT[1];
+                                        const int n1 = UNIT[2];
+                                        T *V2 = W + n1 * s1;
+                                        // the first stage reads the staged block (shared memory) or
+                                        // the block in global memory: one call site for each, so
+                                        // each is compiled for its own address space
                                         if (in0 == PSI)
-                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
-                                                                     OPOFF, ops, PSI, 0, W1, s1, nullptr);
+                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], n1,
+                                                                     UOFF, ops, PSI, 0, W1, s1, nullptr);
                                         else
-                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
-                                                                     OPOFF, ops, xin, 0, W1, s1, nullptr);
+                                                grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], n1,
+                                                                     UOFF, ops, xin, 0, W1, s1, nullptr);
                                         __syncthreads();
                                         grouped_stage<false, NW>(ax[1], w1, ext[ax[1]], dn[ax[1]], g,
-                                                             OPOFF + kGMax, ops, W1, s1, W2, s2, PREF);
+                                                             OPOFF + kGMax, ops, W1, s1, V2, s2, PREF,
+                                                             nullptr, 0, AIDX);
                                         __syncthreads();
-                                        // stage 3 reads W2 only: W1's share is its scratch
-                                        grouped_stage<true, NW>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
-                                                            OPOFF + 2 * kGMax, ops, W2, s2, OUT, 0,
-                                                            nullptr, W1, G * s1);
+                                        // stage 3 reads V2 only: the larger free region (the
+                                        // first-stage results or the tail) is its scratch
+                                        const int used = n1 * s1 + g * s2;
+                                        if (n1 * s1 >= C::kW - used)
+                                                grouped_stage<true, NW>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
+                                                                    OPOFF + 2 * kGMax, ops, V2, s2, OUT, 0,
+                                                                    nullptr, W1, n1 * s1);
+                                        else
+                                                grouped_stage<true, NW>(ax[2], w2, ext[ax[2]], dn[ax[2]], g,
+                                                                    OPOFF + 2 * kGMax, ops, V2, s2, OUT, 0,
+                                                                    nullptr, W + used, C::kW - used);
                                 } else {
+                                        g = cand;
                                         if (in0 == PSI)
                                                 grouped_stage<false, NW>(ax[0], w0, ext[ax[0]], dn[ax[0]], g,
                                                                      OPOFF, ops, PSI, 0, W1, s1, PREF);
@@ -1123,7 +1171,7 @@ static const int kOrders2[2][2] = {{0, 1}, {1, 0}};
 // repeated for every tile along it.  s1, s2: per-tile sizes of the first
 // two intermediates.
 static double seq_cost(const int *seq, int nst, const int *o, const int *n, const int *ext,
-                       const int *nt, int64_t *s1, int64_t *s2)
+                       const int *nt, int64_t *s1, int64_t *s2, double s1scale = 1.0)
 {
         double fl = 0;
         bool done[3] = {false, false, false};
@@ -1135,7 +1183,7 @@ static double seq_cost(const int *seq, int nst, const int *o, const int *n, cons
                         if (j == a) continue;
                         f *= done[j] ? (double) n[j] : (double) o[j] * nt[j];
                 }
-                fl += f;
+                fl += s == 0 ? s1scale * f : f;
                 done[a] = true;
                 wt[a] = ext[a];
                 if (s == 0) *s1 = wt[0] * wt[1] * wt[2];
@@ -1150,7 +1198,8 @@ static double seq_cost(const int *seq, int nst, const int *o, const int *n, cons
 // with M and N padded to the 8 of an mma.m8n8k4 tile and K to its 4, per
 // tile (extent ext) times the number of tiles.  Thin tiles and small dims
 // cost what they occupy on the pipe, not their FLOPs.
-static double tile_cost(const int *seq, int nst, const int *o, const int *ext, const int *nt)
+static double tile_cost(const int *seq, int nst, const int *o, const int *ext, const int *nt,
+                        double s1scale = 1.0)
 {
         auto p8 = [](int64_t x) { return (double) ((x + 7) / 8 * 8); };
         auto p4 = [](int64_t x) { return (double) ((x + 3) / 4 * 4); };
@@ -1170,7 +1219,7 @@ static double tile_cost(const int *seq, int nst, const int *o, const int *ext, c
                         m = p8(cur[0] * cur[1]);
                         n = p8(rows);
                 }
-                c += 2.0 * m * n * p4(cur[a]);
+                c += (s == 0 ? s1scale : 1.0) * 2.0 * m * n * p4(cur[a]);
                 cur[a] = rows;
         }
         return c * nt[0] * nt[1] * nt[2];
@@ -1183,9 +1232,12 @@ static double tile_cost(const int *seq, int nst, const int *o, const int *ext, c
 // For the contraction-ordered kernel (v2) the intermediates take their padded
 // sizes, and an old block larger than psi_cap (padded) is read in place,
 // which needs a sequence that starts on memory axis 0.
+// Terms sorted by their operator on memory axis dax share the first stage
+// when the sequence starts there (three-operator steps, heff_kernel): that
+// stage then costs dfrac of its per-term work.
 static int choose_seq(int nst, const int *o, const int *n, const int *ext, const int *nt,
                       int w_cap, double *fl_out, double *pc_out, int seq_out[3], bool ordered = false,
-                      int psi_cap = 0)
+                      int psi_cap = 0, int dax = -1, double dfrac = 1.0)
 {
         static const int perms3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
                                          {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
@@ -1196,7 +1248,8 @@ static int choose_seq(int nst, const int *o, const int *n, const int *ext, const
         for (int q = 0; q < np; ++q) {
                 const int *seq = nst == 3 ? perms3[q] : perms2[q];
                 int64_t s1 = 0, s2 = 0;
-                const double fl = seq_cost(seq, nst, o, n, ext, nt, &s1, &s2);
+                const double s1scale = (!ordered && nst == 3 && seq[0] == dax) ? dfrac : 1.0;
+                const double fl = seq_cost(seq, nst, o, n, ext, nt, &s1, &s2, s1scale);
                 if (ordered) {
                         const int s0 = seq[0], q1 = seq[1], q2 = nst == 3 ? seq[2] : 3 - seq[0] - seq[1];
                         const int64_t psz = (int64_t) v2::staged_ld(o[s0]) * o[q1] * o[q2];
@@ -1205,7 +1258,7 @@ static int choose_seq(int nst, const int *o, const int *n, const int *ext, const
                         s2 = nst == 3 ? (int64_t) v2::staged_ld(o[q2]) * ext[s0] * ext[q1] : 0;
                 }
                 if (s1 + s2 > w_cap) continue;
-                const double pc = tile_cost(seq, nst, o, ext, nt);
+                const double pc = tile_cost(seq, nst, o, ext, nt, s1scale);
                 if (best < 0 || pc < bpc) { best = q; bfl = fl; bpc = pc; }
         }
         if (best < 0) return -1;
@@ -1334,7 +1387,28 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                         const int t1 = (int) hp.tasks.size();
                         if (t1 > t0) {
                                 const int4 eo4 = hp.edims[ob];
-                                ptmp.push_back({ob, t0, t1, {eo4.x, eo4.y, eo4.z}});
+                                int dax = -1;
+                                double dfrac = 1.0;
+                                if (nops == 3) {
+                                        // the axis with the fewest distinct operator blocks;
+                                        // the pair's terms sorted by it (stable)
+                                        std::vector<int64_t> v(t1 - t0);
+                                        for (int ax = 0; ax < 3; ++ax) {
+                                                for (int t = t0; t < t1; ++t) v[t - t0] = hp.tasks[t].op_off[ax];
+                                                std::sort(v.begin(), v.end());
+                                                const double nd = (double) (std::unique(v.begin(), v.end()) -
+                                                                            v.begin());
+                                                if (dax < 0 || nd / (t1 - t0) < dfrac) {
+                                                        dax = ax;
+                                                        dfrac = nd / (t1 - t0);
+                                                }
+                                        }
+                                        std::stable_sort(hp.tasks.begin() + t0, hp.tasks.begin() + t1,
+                                                         [dax](const HeffTask &a, const HeffTask &b) {
+                                                                 return a.op_off[dax] < b.op_off[dax];
+                                                         });
+                                }
+                                ptmp.push_back({ob, t0, t1, {eo4.x, eo4.y, eo4.z}, dax, dfrac});
                         }
                 }
                 blocks_pairs[nb] = std::move(ptmp);
@@ -1464,7 +1538,7 @@ int tile_plan(HostPlan &hp, int cfg)
                                 int seq[3];
                                 double fl, pc;
                                 if (choose_seq(nops, ptmp[q].eo, en, ext, nt, kc.w_cap, &fl, &pc, seq,
-                                               kc.v2 != 0, kc.psi_cap) != 0) {
+                                               kc.v2 != 0, kc.psi_cap, ptmp[q].dax, ptmp[q].dfrac) != 0) {
                                         ok = false;
                                         break;
                                 }
@@ -1502,7 +1576,9 @@ int tile_plan(HostPlan &hp, int cfg)
                                 int seq[3];
                                 for (int st = 0; st < 3; ++st) seq[st] = (best_seqs[q] >> (2 * st)) & 3;
                                 int64_t s1, s2;
-                                pfl[q] = seq_cost(seq, nops, ptmp[q].eo, en, ext, nt, &s1, &s2) *
+                                const double s1scale = (!kc.v2 && nops == 3 && seq[0] == ptmp[q].dax)
+                                                               ? ptmp[q].dfrac : 1.0;
+                                pfl[q] = seq_cost(seq, nops, ptmp[q].eo, en, ext, nt, &s1, &s2, s1scale) *
                                          (ptmp[q].t1 - ptmp[q].t0);
                         }
                         flops_exec += best_fl;

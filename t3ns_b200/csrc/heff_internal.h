@@ -58,10 +58,15 @@ constexpr int kV2First = 3;   // configurations kV2First.. run heff_v2_kernel
 extern const KernelCfg kCfgs[kNumCfgs];
 
 // One (new, old) pair before tiling: its terms and the old block's dims.
+// The terms are sorted by their operator block on memory axis dax, the axis
+// with the fewest distinct operator blocks (dfrac = distinct / terms): a
+// sequence that starts on dax computes each distinct first-stage result once.
 struct PairTmp {
         int ob;
         int t0, t1;
         int eo[3];
+        int dax;
+        double dfrac;
 };
 
 // The pairs and work units of a plan tiled for one kernel configuration.

@@ -70,6 +70,38 @@ def emulate_blocks(s, plan, x, blocks):
     return out
 
 
+def shared_flops_lower_bound(plan):
+    """Smallest FLOP count any contraction sequence can execute for the
+    plan's terms when the terms of a pair that apply the same first-stage
+    operator share that stage's result (the kernel's grouping, untiled):
+    per pair, the minimum over the sequences of (first stage x distinct
+    first-stage operators + the other stages x terms)."""
+    import itertools
+    pairs = plan["plan.pairs"].reshape(-1, 4)
+    edims = plan["plan.edims"].reshape(-1, 3).astype(np.float64)
+    offs = plan["plan.op_off"].reshape(-1, 3)
+    ptr = plan["plan.pair_ptr"]
+    total = 0.0
+    for nb in range(len(ptr) - 1):
+        dn = edims[nb]
+        for p in range(ptr[nb], ptr[nb + 1]):
+            old, axes, t0, t1 = (int(v) for v in pairs[p])
+            nst = (axes >> 6) & 3
+            do = edims[old]
+            best = None
+            for seq in itertools.permutations(range(3), nst):
+                w = do.copy()
+                cost = 0.0
+                for k, a in enumerate(seq):
+                    f = 2.0 * dn[a] * np.prod(w)
+                    w[a] = dn[a]
+                    n = len(np.unique(offs[t0:t1, a])) if (k == 0 and nst == 3) else t1 - t0
+                    cost += f * n
+                best = cost if best is None else min(best, cost)
+            total += best
+    return total
+
+
 def reference_block(s, y, nb):
     boff = s["beginblock"].astype(np.int64)
     return y[boff[nb]:boff[nb + 1]]
