@@ -215,31 +215,36 @@ def run_engine(args, rank, world):
     t_total = float(sum(t_steps))
     launches = plan.last_launches() * args.steps
 
-    # split precision (3xTF32) on the same step: time, and error against FP64
-    from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_FP64
+    # split precisions (3xTF32, BF16x3) on the same step: time, and error
+    # against FP64
+    from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_BF16X3, T3NS_PREC_FP64
     y64 = y.clone()
-    plan.set_precision(T3NS_PREC_3XTF32)
-    if args.split_kernel_config is None:
-        split_tune = plan.autotune(reps=1)
-    else:
-        split_tune = None
-        plan.set_config(args.split_kernel_config)
-    for _ in range(args.warmup):
-        plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
-    torch.cuda.synchronize()
-    split_times = []
-    for _ in range(args.steps):
-        flush.fill_(1)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
-        e1.record(stream)
-        split_times.append((e0, e1))
-    torch.cuda.synchronize()
-    t_split = float(sum(a.elapsed_time(b) * 1e-3 for a, b in split_times))
-    split_err = float((y - y64).norm() / y64.norm())
-    split_cfg = plan.config()
+
+    def time_precision(prec):
+        plan.set_precision(prec)
+        if args.split_kernel_config is None:
+            tune = plan.autotune(reps=1)
+        else:
+            tune = None
+            plan.set_config(args.split_kernel_config)
+        for _ in range(args.warmup):
+            plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize()
+        t = float(sum(a.elapsed_time(b) * 1e-3 for a, b in ts))
+        return t, float((y - y64).norm() / y64.norm()), plan.config(), tune
+
+    t_split, split_err, split_cfg, split_tune = time_precision(T3NS_PREC_3XTF32)
+    t_bf, bf_err, bf_cfg, bf_tune = time_precision(T3NS_PREC_BF16X3)
     plan.set_precision(T3NS_PREC_FP64)
     if args.kernel_config is None:
         plan.autotune(reps=1, force=False)
@@ -266,7 +271,7 @@ def run_engine(args, rank, world):
     assert err < 1e-12, err
 
     # every rank takes this collective, in the same order
-    t_total, t_e2e, t_split = max_over_ranks([t_total, t_e2e, t_split], world, "cuda")
+    t_total, t_e2e, t_split, t_bf = max_over_ranks([t_total, t_e2e, t_split, t_bf], world, "cuda")
     if rank != 0:
         return None
     flops = st["flops_ref"]
@@ -296,6 +301,11 @@ def run_engine(args, rank, world):
                             "autotune_ms": split_tune,
                             "arithmetic": "3xTF32 products of pre-split {hi, lo} TF32 pairs, "
                                           "FP32 accumulation"},
+        "bf16x3": {"value": flops * args.steps * world / t_bf / 1e12, "unit": UNIT,
+                   "ms_per_step": 1e3 * t_bf / args.steps, "speedup_vs_fp64": t_total / t_bf,
+                   "rel_err_vs_fp64": bf_err, "kernel_config": bf_cfg, "autotune_ms": bf_tune,
+                   "arithmetic": "3 BF16 products of pre-split {hi, lo} BF16 pairs "
+                                 "(4 bytes an element), FP32 accumulation"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -537,7 +547,8 @@ def microbench_d1024(args, peak, reps=None):
     FP64; CUDA events, L2 flushed between iterations."""
     import torch
 
-    from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_FP64, HeffPlan, StepDesc
+    from t3ns_b200.native import (T3NS_PREC_3XTF32, T3NS_PREC_BF16X3, T3NS_PREC_FP64, HeffPlan,
+                                  StepDesc)
     from t3ns_b200.stepfile import read_step
     files = sorted(glob.glob(os.path.join(DEFAULT_WORKLOAD_DIR, MICRO_PATTERN)))
     if not files:
@@ -584,6 +595,11 @@ def microbench_d1024(args, peak, reps=None):
         tsp = timed(lambda: plan.matvec_device(x.data_ptr(), y.data_ptr(), sh))
         err = float((y - y64).norm() / y64.norm())
         cfgsp = plan.config()
+        plan.set_precision(T3NS_PREC_BF16X3)
+        btune = plan.autotune(reps=1)
+        tbf = timed(lambda: plan.matvec_device(x.data_ptr(), y.data_ptr(), sh))
+        bf_err = float((y - y64).norm() / y64.norm())
+        cfgbf = plan.config()
         plan.set_precision(T3NS_PREC_FP64)
         plan.close()
         out.append({
@@ -598,7 +614,9 @@ def microbench_d1024(args, peak, reps=None):
             "split_3xtf32": {"ms": tsp, "tflops": F / tsp / 1e9, "kernel_config": cfgsp,
                              "autotune_ms": stune, "speedup_vs_fp64": t64 / tsp,
                              "rel_err_vs_fp64": err},
-            "bf16x3": "not built",
+            "bf16x3": {"ms": tbf, "tflops": F / tbf / 1e9, "kernel_config": cfgbf,
+                       "autotune_ms": btune, "speedup_vs_fp64": t64 / tbf,
+                       "rel_err_vs_fp64": bf_err},
         })
         del x, y, y64
         torch.cuda.empty_cache()

@@ -33,8 +33,11 @@ extern "C" {
 #define T3NS_E_EIG -6      /* the subspace eigensolver did not converge      */
 
 /* Matvec arithmetic.  FP64 computes every product and sum in double.
- * The split modes (3xTF32, BF16x3) run the block contractions on the tensor
- * cores with FP32 accumulation; results stay double in HBM. */
+ * The split modes run the block contractions on the tensor cores as three
+ * products of {hi, lo} operand pairs with FP32 accumulation; results stay
+ * double in HBM.  3xTF32: TF32 pairs (about 2^-22 relative per product, every
+ * kernel configuration).  BF16x3: BF16 pairs, half the operand bytes (about
+ * 2^-16 relative per product, configurations 0-2). */
 #define T3NS_PREC_FP64 0
 #define T3NS_PREC_3XTF32 1
 #define T3NS_PREC_BF16X3 2
@@ -135,8 +138,9 @@ int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag);
  * tiles, 2 = one 768-thread CTA per SM (more warps, fewer registers a thread)
  * with mid-size tiles; 3 and 4 = the contraction-ordered kernel (every stage
  * contracts the fastest axis of its input, operators transposed on the
- * device) with 768 and 512 threads, FP64 only.  Each has its own tiling of the
- * plan (built on first use). */
+ * device) with 768 and 512 threads, FP64 and 3xTF32.  Each has its own tiling
+ * of the plan (built on first use).  A BF16x3 plan runs configurations 0-2
+ * only (selecting 3 or 4 is an error, T3NS_E_ARG). */
 #define T3NS_NUM_CONFIGS 5
 int t3ns_heff_set_config(t3ns_heff *h, int config);
 int t3ns_heff_get_config(const t3ns_heff *h);

@@ -117,6 +117,18 @@ def structure_only(path, out, compress=False):
     write_step(out, rec, compress_above=(1 << 20) if compress else None)
 
 
+def structure_from_capture(t3c, sched, out, compress=True):
+    """Joins a structure capture (t3ns_run --capture-structure: the step's
+    structure with ops{i}.tel_len) and its compiled schedule (the .sched
+    file, records my.*) into one structure-only step file with the
+    schedule under the reference's names (sr.*)."""
+    rec = dict(read_step(t3c))
+    for k, v in read_step(sched).items():
+        if k.startswith("my.") and k != "my.nr_qnB":
+            rec["sr." + k[3:]] = v
+    write_step(out, rec, compress_above=(1 << 20) if compress else None)
+
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 REF = os.path.join(HERE, "_ref")

@@ -125,6 +125,8 @@ static void dump_symsecs(const char *pre, const struct symsecs *ss)
         if (ss->dims) cap_i32(nm, ss->nrSecs, ss->dims);
 }
 
+static int opt_structure_only;          /* dump operator lengths, not values */
+
 static void dump_rops(int i, const struct rOperators *op)
 {
         char nm[64];
@@ -159,7 +161,12 @@ static void dump_rops(int i, const struct rOperators *op)
                 pt += sz;
         }
         cap_i32(NM("beginblock"), nbb, bb);
-        cap_f64(NM("tel"), ntel, tel);
+        if (opt_structure_only) {
+                const int64_t len = ntel;
+                cap_i64(NM("tel_len"), 1, &len);
+        } else {
+                cap_f64(NM("tel"), ntel, tel);
+        }
         free(bb);
         free(tel);
 #undef NM
@@ -342,6 +349,117 @@ static int capture_step(struct Heffdata *hd, double *guess, int size,
         fflush(stdout);
         return ret;
 }
+
+/* --capture-structure DIR (either build): for every selected step, the step's
+ * structure only -- site tensor blocks, symsecs, the operator sets' block
+ * structure with their element counts (ops{i}.tel_len) instead of values,
+ * the merge instruction set -- to DIR/step_NNN.t3c, and the schedule the
+ * product's compiler builds for it (bit-identical to the reference's replay
+ * schedule, which the drop-in tests check pair by pair) to
+ * DIR/step_NNN.sched; the Davidson solve is skipped (the step keeps the
+ * driver's guess).  The benchmark workloads are made from these pairs
+ * (oracle/captures.py): in the drop-in build the initial operators and the
+ * updates run on the GPU, which makes large bond dimensions reachable. */
+static const char *opt_capture_structure;
+
+static void capture_structure(const struct Heffdata *hd, int size)
+{
+        char path[4096];
+        snprintf(path, sizeof path, "%s/step_%03d.t3c", opt_capture_structure, opt_step_counter);
+        cap_fp = fopen(path, "wb");
+        if (!cap_fp) { perror(path); exit(EXIT_FAILURE); }
+        fwrite("T3NSCAP1", 1, 8, cap_fp);
+        const struct siteTensor *st = &hd->siteObject;
+        cap_int("step", opt_step_counter);
+        cap_int("isdmrg", hd->isdmrg);
+        cap_int("nrsites", st->nrsites);
+        cap_i32("sites", st->nrsites, st->sites);
+        cap_int("posB", hd->posB);
+        cap_i32("rOperators_on_site", 3, hd->rOperators_on_site);
+        cap_int("nrblocks", st->nrblocks);
+        cap_i64("qnumbers", (int64_t) st->nrblocks * st->nrsites, (const int64_t *) st->qnumbers);
+        cap_i32("beginblock", st->nrblocks + 1, st->blocks.beginblock);
+        cap_int("nrSyms", bookie.nrSyms);
+        cap_i32("sgs", bookie.nrSyms, (const int *) bookie.sgs);
+        cap_int("MAX_SYMMETRIES", MAX_SYMMETRIES);
+        char nm[64];
+        for (int i = 0; i < st->nrsites; ++i)
+                for (int j = 0; j < 3; ++j) {
+                        snprintf(nm, sizeof nm, "symarr%d%d", i, j);
+                        dump_symsecs(nm, &hd->symarr[i][j]);
+                }
+        dump_symsecs("MPOsymsec", &hd->MPOsymsec);
+        opt_structure_only = 1;
+        for (int i = 0; i < (hd->isdmrg ? 2 : 3); ++i) dump_rops(i, &hd->Operators[i]);
+        opt_structure_only = 0;
+        const struct instructionset *is = &hd->iset;
+        cap_int("iset.nr_instr", is->nr_instr);
+        cap_int("iset.step", is->step);
+        int *ins = malloc(sizeof *ins * 3 * (size_t) (is->nr_instr + 1));
+        double *pr = malloc(sizeof *pr * (size_t) (is->nr_instr + 1));
+        for (int k = 0; k < is->nr_instr; ++k) {
+                for (int c = 0; c < 3; ++c) ins[3 * k + c] = is->instr[k].instr[c];
+                pr[k] = is->instr[k].pref;
+        }
+        cap_i32("iset.instr", 3L * is->nr_instr, ins);
+        cap_f64("iset.pref", is->nr_instr, pr);
+        free(ins);
+        free(pr);
+        cap_int("iset.nrMPOc", is->nrMPOc);
+        cap_i32("iset.MPOc", is->nrMPOc, is->MPOc);
+        cap_i32("iset.MPOc_beg", is->nrMPOc + 1, is->MPOc_beg);
+        fclose(cap_fp);
+        cap_fp = NULL;
+
+        static int (*wr)(const struct Heffdata *, const char *);
+        if (!wr) {
+                void *h = opt_schedule_lib ? dlopen(opt_schedule_lib, RTLD_NOW | RTLD_LOCAL)
+                                           : RTLD_DEFAULT;
+                wr = h ? (int (*)(const struct Heffdata *, const char *))
+                                 dlsym(h, "t3ns_dropin_schedule_write")
+                       : NULL;
+                if (!wr) { fprintf(stderr, "no t3ns_dropin_schedule_write\n"); exit(EXIT_FAILURE); }
+        }
+        char sp[4096];
+        snprintf(sp, sizeof sp, "%s/step_%03d.sched", opt_capture_structure, opt_step_counter);
+        if (wr(hd, sp) != 0) { fprintf(stderr, "schedule write failed\n"); exit(EXIT_FAILURE); }
+        ++opt_captured;
+        fprintf(stdout, "CAPTURED_STRUCTURE %s size %d blocks %d\n", path, size, st->nrblocks);
+        fflush(stdout);
+}
+
+#ifdef T3NS_RUN_DROPIN
+/* In the drop-in build only the structure capture interposes the drop-in's
+ * sparse_eigensolve. */
+int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
+                      int keep_deflate, double tol, int max_its,
+                      const double *diagonal,
+                      void (*matvec)(const double *, double *, void *),
+                      void *vdat, const char solver[])
+{
+        static eig_fn real_eig;
+        if (!real_eig) real_eig = (eig_fn) dlsym(RTLD_NEXT, "sparse_eigensolve");
+        if (!real_eig) { fprintf(stderr, "sparse_eigensolve not found\n"); exit(EXIT_FAILURE); }
+        int ret = 0;
+        if (opt_capture_structure) {
+                if (opt_captured < opt_capture_limit && size <= opt_capture_max &&
+                    size >= opt_capture_min) {
+                        capture_structure((const struct Heffdata *) vdat, size);
+                        if (opt_capture_stop && opt_captured >= opt_capture_limit) {
+                                printf("CAPTURE_DONE\n");
+                                fflush(stdout);
+                                _exit(0);
+                        }
+                }
+                *energy = 0;
+        } else {
+                ret = real_eig(result, energy, size, max_vecs, keep_deflate, tol, max_its,
+                               diagonal, matvec, vdat, solver);
+        }
+        ++opt_step_counter;
+        return ret;
+}
+#endif
 
 #ifndef T3NS_RUN_DROPIN
 static void dump_siteTensor(const char *pre, const struct siteTensor *t)
@@ -622,7 +740,27 @@ int sparse_eigensolve(double *result, double *energy, int size, int max_vecs,
         const int want = opt_capture_dir && opt_captured < opt_capture_limit &&
                 size <= opt_capture_max && size >= opt_capture_min;
         int ret = 0;
-        if (want) {
+        if (opt_capture_structure) {
+                if (opt_captured < opt_capture_limit && size <= opt_capture_max &&
+                    size >= opt_capture_min) {
+                        /* one matvec builds the replay schedule that
+                         * destroy_Heffdata frees */
+                        double *tmp = malloc(sizeof *tmp * (size_t) size);
+                        matvec(result, tmp, vdat);
+                        free(tmp);
+                        capture_structure((const struct Heffdata *) vdat, size);
+                        if (opt_capture_stop && opt_captured >= opt_capture_limit) {
+                                printf("CAPTURE_DONE\n");
+                                fflush(stdout);
+                                _exit(0);
+                        }
+                } else {
+                        double *tmp = malloc(sizeof *tmp * (size_t) size);
+                        matvec(result, tmp, vdat);
+                        free(tmp);
+                }
+                *energy = 0;
+        } else if (want) {
                 /* runs the reference Davidson in place on result */
                 ret = capture_step((struct Heffdata *) vdat, result, size, diagonal,
                                    max_vecs, keep_deflate, tol, max_its, real_eig,
@@ -702,6 +840,7 @@ int main(int argc, char **argv)
                 else if (!strcmp(a, "--ts") && v) { ts = v; ++i; }
                 else if (!strcmp(a, "--init") && v) { init = v[0]; ++i; }
                 else if (!strcmp(a, "--capture") && v) { opt_capture_dir = v; ++i; }
+                else if (!strcmp(a, "--capture-structure") && v) { opt_capture_structure = v; ++i; }
                 else if (!strcmp(a, "--capture-max") && v) { opt_capture_max = atol(v); ++i; }
                 else if (!strcmp(a, "--capture-min") && v) { opt_capture_min = atol(v); ++i; }
                 else if (!strcmp(a, "--capture-limit") && v) { opt_capture_limit = atoi(v); ++i; }

@@ -47,11 +47,13 @@ def build_engine(force: bool = False) -> str:
     if force or _stale(out, deps):
         from concurrent.futures import ThreadPoolExecutor
         objs = [os.path.join(LIBDIR, os.path.basename(s) + ".o") for s in srcs]
+        headers = [d for d in deps if d not in srcs]
+        # an object is rebuilt when its source or any header is newer
         cmds = [[NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                  "-Xptxas", "-warn-spills", "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
-                for s, o in zip(srcs, objs)]
+                for s, o in zip(srcs, objs) if force or _stale(o, [s, *headers])]
         # the translation units compile independently (heff.cu dominates)
-        with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
             list(ex.map(_run, cmds))
         _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart_static", "-lrt", "-ldl",
               "-lpthread"])

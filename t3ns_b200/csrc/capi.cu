@@ -137,12 +137,23 @@ static int upload_tiles(t3ns_heff *h, int cfg)
 // matvec.
 static int setup_precision(t3ns_heff *h, int precision)
 {
-        if (precision == T3NS_PREC_BF16X3)
-                return set_error(T3NS_E_ARG, "BF16x3 matvec is not built in this library "
-                                             "(use T3NS_PREC_3XTF32)");
-        if (precision != T3NS_PREC_FP64 && precision != T3NS_PREC_3XTF32)
+        if (precision != T3NS_PREC_FP64 && precision != T3NS_PREC_3XTF32 &&
+            precision != T3NS_PREC_BF16X3)
                 return set_error(T3NS_E_ARG, "unknown precision");
         DevicePlan &dp = h->dp;
+        if (precision == T3NS_PREC_BF16X3) {
+                // BF16x3 runs on the configurations 0-2 (heff_kernel)
+                if (kCfgs[dp.active].v2) {
+                        T3NS_TRY(upload_tiles(h, 0));
+                        dp.active = 0;
+                }
+                if (!dp.ops_bf16) {
+                        T3NS_TRY(dev_alloc(h, &dp.ops_bf16, (size_t) h->hp.op_elems));
+                        T3NS_TRY(dev_alloc(h, &dp.x_bf16, (size_t) h->hp.size));
+                        T3NS_TRY(convert_to_bf16_pairs(dp.ops, dp.ops_bf16, h->hp.op_elems, h->stream));
+                        T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+                }
+        }
         if (precision == T3NS_PREC_3XTF32 && !dp.ops_split) {
                 T3NS_TRY(dev_alloc(h, &dp.ops_split, (size_t) h->hp.op_elems));
                 T3NS_TRY(dev_alloc(h, &dp.x_split, (size_t) h->hp.size));
@@ -300,6 +311,8 @@ int t3ns_heff_set_config(t3ns_heff *h, int config)
 {
         if (!h) return set_error(T3NS_E_ARG, "null plan");
         if (config < 0 || config >= kNumCfgs) return set_error(T3NS_E_ARG, "unknown configuration");
+        if (h->precision == T3NS_PREC_BF16X3 && kCfgs[config].v2)
+                return set_error(T3NS_E_ARG, "BF16x3 runs on configurations 0-2 only");
         T3NS_TRY(upload_tiles(h, config));
         h->dp.active = config;
         return T3NS_OK;
@@ -327,6 +340,7 @@ int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
         int rc = T3NS_OK;
         bool first = true;
         for (int c = 0; c < kNumCfgs && rc == T3NS_OK; ++c) {
+                if (h->precision == T3NS_PREC_BF16X3 && kCfgs[c].v2) continue;
                 rc = t3ns_heff_set_config(h, c);
                 if (rc != T3NS_OK) break;
                 // one untimed run, then `reps` timed ones

@@ -39,7 +39,11 @@ static constexpr int kRedThreads = 256;
 static constexpr int kChunk = 8;         // basis columns per register pass
 static constexpr double kDiagCutoff = 1e-12;
 static constexpr int kMaxVecs = 32;      // largest Davidson subspace
-static constexpr double kStallLevel = 1e-4;   // see davidson_core's `stall`
+// see davidson_core's `stall`: the residual level below which a split-precision
+// solve may level off, relative to max(1, |energy|): 3xTF32 matvecs are
+// accurate to ~2e-6 relative, BF16x3 to ~1e-5 (more on small steps)
+static constexpr double kStallLevel = 1e-4;
+static constexpr double kStallLevelBf16 = 1e-2;
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -454,16 +458,17 @@ static int alloc_basis(DavidsonBuffers &b, int64_t n, int max_vecs)
 using DevMatvec = std::function<int(const double *, double *, cudaStream_t)>;
 
 // stall > 0: also stop (returning 2) once the residual is below
-// kStallLevel * max(1, |energy|) -- the region where the split-precision
-// matvec's rounding (~2e-6 relative) can level it off -- and has not fallen
-// below 0.9 of its best value for `stall` iterations.
+// stall_level * max(1, |energy|) -- the region where the split-precision
+// matvec's rounding can level it off -- and has not fallen below 0.9 of its
+// best value for `stall` iterations.
 // mv_err (optional): the matvec kernel's device error status; it is read back
 // with the iteration's scalars and a non-zero value ends the solve with
 // T3NS_E_DEVICE instead of continuing on a wrong product.
 static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, double *energy,
                          int max_vecs, int keep, double tol, int max_its, const double *d_diag,
                          t3ns_davidson_info *info, cudaStream_t s, int stall = 0,
-                         bool use_graphs = false, const int *mv_err = nullptr)
+                         bool use_graphs = false, const int *mv_err = nullptr,
+                         double stall_level = kStallLevel)
 {
         const auto t_start = std::chrono::steady_clock::now();
         if (max_vecs > kMaxVecs || keep > 4 || keep < 1 || keep >= max_vecs || max_vecs < 3)
@@ -612,7 +617,7 @@ static int davidson_core(int64_t n, const DevMatvec &matvec, double *d_result, d
                         best_res = res;
                         since_best = 0;
                 } else if (stall > 0 && ++since_best >= stall &&
-                           res < kStallLevel * std::max(1.0, fabs(b.host_scal[3]))) {
+                           res < stall_level * std::max(1.0, fabs(b.host_scal[3]))) {
                         stalled = true;
                 }
                 const double theta = b.host_scal[3];
@@ -653,11 +658,16 @@ int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
                 return davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy,
                                      max_vecs, keep, tol, max_its, d_diag, info, s, 0, graphs,
                                      h->dp.err);
-        // split-precision iterations, then FP64 defect correction from their vector
+        // split-precision iterations, then FP64 defect correction from their
+        // vector; the split phase leaves at least a quarter of the iterations
+        // (and 10) to the FP64 phase
         t3ns_davidson_info i1{}, i2{};
         const auto t0 = std::chrono::steady_clock::now();
+        const int split_its = std::max(1, max_its - std::max(10, max_its / 4));
+        const double level = h->precision == T3NS_PREC_BF16X3 ? kStallLevelBf16 : kStallLevel;
         int rc = davidson_core(h->hp.size, matvec_in(h->precision), d_result, energy, max_vecs,
-                               keep, tol, max_its, d_diag, &i1, s, /*stall=*/4, graphs, h->dp.err);
+                               keep, tol, split_its, d_diag, &i1, s, /*stall=*/4, graphs, h->dp.err,
+                               level);
         if (rc < 0) return rc;
         rc = davidson_core(h->hp.size, matvec_in(T3NS_PREC_FP64), d_result, energy, max_vecs,
                            keep, tol, std::max(max_its - i1.iterations, 2), d_diag, &i2, s, 0,

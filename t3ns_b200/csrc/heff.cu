@@ -33,6 +33,8 @@
 //     the last scales by the term prefactor, so the last stage is a plain
 //     reduction over the group inside each warp (single owner per output
 //     element: no atomics).
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <bitset>
 #include <cmath>
@@ -545,6 +547,134 @@ __device__ __forceinline__ void warp_tile_tf32x3(float (&d)[RM][RN][4], const fl
         }
 }
 
+// ---------------------------------------------------------------------------
+// BF16x3 stages: x = hi + lo with hi = bf16(x), lo = bf16(x - hi) (16
+// significant bits together), x*y ~ lo_x*hi_y + hi_x*lo_y + hi_x*hi_y on the
+// BF16 tensor pipe (mma.m16n8k16), FP32 accumulation; the dropped lo*lo term
+// and the representation error are ~2^-16 relative.  An element is stored
+// as one 32-bit pair (hi in the low half, lo in the high half): half the
+// bytes of an FP64 or {hi, lo} TF32 operand, and twice the K of a TF32 MMA.
+struct __align__(4) BfPair {
+        uint32_t v;
+};
+
+__device__ __forceinline__ uint32_t bf16_bits(float x)
+{
+        return (uint32_t) __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+
+__device__ __forceinline__ float bf16_value(uint32_t b)
+{
+        return __uint_as_float(b << 16);
+}
+
+__device__ __forceinline__ BfPair split_bf16(float x)
+{
+        const uint32_t hi = bf16_bits(x);
+        return BfPair{hi | (bf16_bits(x - bf16_value(hi)) << 16)};
+}
+
+// D(16x8) += A(16x16) * B(16x8).  Fragments (PTX ISA, mma.m16n8k16 .bf16),
+// with g = lane/4, t = lane%4, each register two K-consecutive elements
+// (the lower K in the low half): a = {A[g][2t..2t+1], A[g+8][2t..2t+1],
+// A[g][2t+8..2t+9], A[g+8][2t+8..2t+9]}, b = {B[2t..2t+1][g],
+// B[2t+8..2t+9][g]}; d as for the TF32 MMA.
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
+{
+        asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
+                     "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                     : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                     : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// hi (sel 0x5410) or lo (sel 0x7632) halves of two K-consecutive pairs
+__device__ __forceinline__ uint32_t pick(uint32_t p0, uint32_t p1, uint32_t sel)
+{
+        return __byte_perm(p0, p1, sel);
+}
+
+// Warp tile of (16*RM) x (8*RN) outputs over BF16 pairs; addressing as
+// warp_tile_tf32x3 (A(m,k) = Ab[arow(m) + k*ak], B(k,n) = Bb[k*bk + bcol(n)]).
+template <int RM, int RN>
+__device__ __forceinline__ void warp_tile_x3(float (&d)[RM][RN][4], const BfPair *Ab, int am,
+                                             int ak, const BfPair *Bb, int bk, int bn,
+                                             const RowSplit &rs, bool split_a, int K, int M, int N,
+                                             int m0, int n0, int g, int t)
+{
+        int ao[RM][2], bo[RN];
+#pragma unroll
+        for (int i = 0; i < RM; ++i)
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                        const int m = m0 + 16 * i + 8 * r + g;
+                        ao[i][r] = m < M ? (int) (split_a ? rs.a_off(m) : (int64_t) m * am) + 2 * t * ak : -1;
+                }
+#pragma unroll
+        for (int j = 0; j < RN; ++j) {
+                const int n = n0 + 8 * j + g;
+                bo[j] = n < N ? (int) (split_a ? (int64_t) n * bn : rs.a_off(n)) + 2 * t * bk : -1;
+        }
+        const uint32_t *A = reinterpret_cast<const uint32_t *>(Ab);
+        const uint32_t *B = reinterpret_cast<const uint32_t *>(Bb);
+        for (int k0 = 0, ka = 0, kb = 0; k0 < K; k0 += 16, ka += 16 * ak, kb += 16 * bk) {
+                // this lane's K indices: k0 + 2t + {0, 1, 8, 9}
+                const int kk = k0 + 2 * t;
+                const bool q0 = kk < K, q1 = kk + 1 < K, q2 = kk + 8 < K, q3 = kk + 9 < K;
+                uint32_t ah[RM][4], al[RM][4], bh[RN][2], bl[RN][2];
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int r = 0; r < 2; ++r) {
+                                const bool ok = ao[i][r] >= 0;
+                                const int o = ao[i][r] + ka;
+                                const uint32_t e0 = (ok && q0) ? A[o] : 0u;
+                                const uint32_t e1 = (ok && q1) ? A[o + ak] : 0u;
+                                const uint32_t e2 = (ok && q2) ? A[o + 8 * ak] : 0u;
+                                const uint32_t e3 = (ok && q3) ? A[o + 9 * ak] : 0u;
+                                ah[i][r] = pick(e0, e1, 0x5410);
+                                al[i][r] = pick(e0, e1, 0x7632);
+                                ah[i][r + 2] = pick(e2, e3, 0x5410);
+                                al[i][r + 2] = pick(e2, e3, 0x7632);
+                        }
+#pragma unroll
+                for (int j = 0; j < RN; ++j) {
+                        const bool ok = bo[j] >= 0;
+                        const int o = bo[j] + kb;
+                        const uint32_t f0 = (ok && q0) ? B[o] : 0u;
+                        const uint32_t f1 = (ok && q1) ? B[o + bk] : 0u;
+                        const uint32_t f2 = (ok && q2) ? B[o + 8 * bk] : 0u;
+                        const uint32_t f3 = (ok && q3) ? B[o + 9 * bk] : 0u;
+                        bh[j][0] = pick(f0, f1, 0x5410);
+                        bl[j][0] = pick(f0, f1, 0x7632);
+                        bh[j][1] = pick(f2, f3, 0x5410);
+                        bl[j][1] = pick(f2, f3, 0x7632);
+                }
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) {
+                                mma_bf16(d[i][j], al[i], bh[j]);
+                                mma_bf16(d[i][j], ah[i], bl[j]);
+                                mma_bf16(d[i][j], ah[i], bh[j]);
+                        }
+        }
+}
+
+// the 3xTF32 tile under the common name of the split stages
+template <int RM, int RN>
+__device__ __forceinline__ void warp_tile_x3(float (&d)[RM][RN][4], const float2 *Ab, int am,
+                                             int ak, const float2 *Bb, int bk, int bn,
+                                             const RowSplit &rs, bool split_a, int K, int M, int N,
+                                             int m0, int n0, int g, int t)
+{
+        warp_tile_tf32x3<RM, RN>(d, Ab, am, ak, Bb, bk, bn, rs, split_a, K, M, N, m0, n0, g, t);
+}
+
+__device__ __forceinline__ void store_out(BfPair *p, float v, float sc, bool acc)
+{
+        *p = split_bf16(sc * v);   // intermediates: split once, here
+}
+
 __device__ __forceinline__ void store_out(float2 *p, float v, float sc, bool acc)
 {
         *p = split_tf32(sc * v);   // intermediates: split once, here
@@ -558,11 +688,11 @@ __device__ __forceinline__ void store_out(float *p, float v, float sc, bool acc)
 // The grouped stage of the FP64 path for pre-split operands.  The GEMM is
 // taken in the orientation that puts the larger of M and N on the tile's
 // 16-row side.
-template <bool ACC, int RM, int RN, int NW, class OutT>
+template <bool ACC, int RM, int RN, int NW, class E, class OutT>
 __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows, int ldop, int G,
                                                   const int64_t *opoff,
-                                                  const float2 *__restrict__ ops,
-                                                  const float2 *in, int in_gs, OutT *out,
+                                                  const E *__restrict__ ops,
+                                                  const E *in, int in_gs, OutT *out,
                                                   int out_gs, const float *scale, bool swap,
                                                   float *scratch, int scratch_cap,
                                                   const int *in_idx)
@@ -615,16 +745,16 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) d[i][j][q] = 0.f;
                 for (int gg = g0; gg < g1; gg += gstep) {
-                        const float2 *op = ops + opoff[gg];
-                        const float2 *tin = in + (!ACC && in_idx ? in_idx[gg] : gg) * in_gs;
-                        const float2 *Ab = ax == 0 ? op : tin;
-                        const float2 *Bb = ax == 0 ? tin : op;
+                        const E *op = ops + opoff[gg];
+                        const E *tin = in + (!ACC && in_idx ? in_idx[gg] : gg) * in_gs;
+                        const E *Ab = ax == 0 ? op : tin;
+                        const E *Bb = ax == 0 ? tin : op;
                         if (swap)
-                                warp_tile_tf32x3<RM, RN>(d, Bb, bn, bk, Ab, ak, 1, rs, false, K, Mt, Nt,
-                                                         m0, n0, g, t);
+                                warp_tile_x3<RM, RN>(d, Bb, bn, bk, Ab, ak, 1, rs, false, K, Mt, Nt,
+                                                     m0, n0, g, t);
                         else
-                                warp_tile_tf32x3<RM, RN>(d, Ab, 1, ak, Bb, bk, bn, rs, true, K, Mt, Nt,
-                                                         m0, n0, g, t);
+                                warp_tile_x3<RM, RN>(d, Ab, 1, ak, Bb, bk, bn, rs, true, K, Mt, Nt,
+                                                     m0, n0, g, t);
                 }
                 const float sc = (!ACC && scale) ? scale[g0] : 1.f;
                 OutT *Cb = out + (ACC ? 0 : g0 * out_gs);
@@ -666,16 +796,17 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
         }
 }
 
-template <bool ACC, int NW, class OutT>
-__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
-                                              const int64_t *opoff, const float2 *__restrict__ ops,
-                                              const float2 *in, int in_gs, OutT *out, int out_gs,
-                                              const float *scale, float2 *scratch = nullptr,
-                                              int scratch_cap = 0, const int *in_idx = nullptr)
+template <bool ACC, int NW, class E, class OutT>
+__device__ __forceinline__ void grouped_stage_split(int ax, const int *w, int rows, int ldop, int G,
+                                                    const int64_t *opoff, const E *__restrict__ ops,
+                                                    const E *in, int in_gs, OutT *out, int out_gs,
+                                                    const float *scale, E *scratch, int scratch_cap,
+                                                    const int *in_idx)
 {
-        // the scratch holds FP32 partial tiles: two per float2 slot
+        // the scratch holds FP32 partial tiles (two per float2 slot, one per
+        // BF16 pair)
         float *fs = reinterpret_cast<float *>(scratch);
-        const int fcap = 2 * scratch_cap;
+        const int fcap = scratch_cap * (int) (sizeof(E) / sizeof(float));
         const int M = ax == 0 ? rows : ax == 1 ? w[0] * w[2] : w[0] * w[1];
         const int N = ax == 0 ? w[1] * w[2] : rows;
         // padded work of the two orientations (16 x 8 granules)
@@ -694,6 +825,29 @@ __device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, in
                                                  out_gs, scale, swap, fs, fcap, in_idx);
 }
 
+// the split-precision stages for the two operand encodings
+template <bool ACC, int NW, class OutT>
+__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
+                                              const int64_t *opoff, const float2 *__restrict__ ops,
+                                              const float2 *in, int in_gs, OutT *out, int out_gs,
+                                              const float *scale, float2 *scratch = nullptr,
+                                              int scratch_cap = 0, const int *in_idx = nullptr)
+{
+        grouped_stage_split<ACC, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
+                                     scratch, scratch_cap, in_idx);
+}
+
+template <bool ACC, int NW, class OutT>
+__device__ __forceinline__ void grouped_stage(int ax, const int *w, int rows, int ldop, int G,
+                                              const int64_t *opoff, const BfPair *__restrict__ ops,
+                                              const BfPair *in, int in_gs, OutT *out, int out_gs,
+                                              const float *scale, BfPair *scratch = nullptr,
+                                              int scratch_cap = 0, const int *in_idx = nullptr)
+{
+        grouped_stage_split<ACC, NW>(ax, w, rows, ldop, G, opoff, ops, in, in_gs, out, out_gs, scale,
+                                     scratch, scratch_cap, in_idx);
+}
+
 // Element types of the kernel: operand storage T, the output tile's
 // accumulator and the term prefactors.
 template <class T>
@@ -708,16 +862,22 @@ struct Elem<float2> {
         using Acc = float;
         using Scale = float;
 };
+template <>
+struct Elem<BfPair> {
+        using Acc = float;
+        using Scale = float;
+};
 
 // Shared buffer capacities (elements) of a configuration for element type T:
 // the output tile is the plan's; the staged block and intermediates take the
-// configuration's bytes (a float2 pair is as wide as a double).
+// configuration's bytes (a float2 pair is as wide as a double, a BF16 pair
+// half as wide, so twice as many fit).
 template <class Cfg, class T>
 struct Caps {
         static constexpr int kOut = Cfg::kOut;
         static constexpr int kPsi = Cfg::kPsi * (int) (sizeof(double) / sizeof(T));
         static constexpr int kW = Cfg::kW * (int) (sizeof(double) / sizeof(T));
-        static_assert(sizeof(T) == sizeof(double), "operands are 8 bytes wide");
+        static_assert(sizeof(double) % sizeof(T) == 0, "operands are 8 or 4 bytes wide");
 };
 
 template <class Cfg, class T>
@@ -1737,6 +1897,29 @@ __global__ void split_tf32_kernel(const double *__restrict__ a, float2 *__restri
         }
 }
 
+// b[i] = {hi, lo}: hi = bf16(a[i]), lo = bf16(a[i] - hi), the remainder
+// taken in FP64.
+__global__ void split_bf16_kernel(const double *__restrict__ a, BfPair *__restrict__ b, int64_t n)
+{
+        for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+             i += (int64_t) gridDim.x * blockDim.x) {
+                const double v = a[i];
+                const uint32_t hi = (uint32_t) __bfloat16_as_ushort(__double2bfloat16(v));
+                const uint32_t lo = (uint32_t) __bfloat16_as_ushort(
+                        __double2bfloat16(v - (double) bf16_value(hi)));
+                b[i] = BfPair{hi | (lo << 16)};
+        }
+}
+
+int convert_to_bf16_pairs(const double *a, void *b, int64_t n, cudaStream_t s)
+{
+        if (n <= 0) return T3NS_OK;
+        const int grid = (int) std::min<int64_t>((n + 255) / 256, 148 * 16);
+        split_bf16_kernel<<<grid, 256, 0, s>>>(a, reinterpret_cast<BfPair *>(b), n);
+        T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
+}
+
 int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s)
 {
         if (n <= 0) return T3NS_OK;
@@ -1781,15 +1964,21 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         const DeviceTiles &dt = dp.tiles[dp.active];
         if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
         const bool split = precision == T3NS_PREC_3XTF32;
+        const bool bf = precision == T3NS_PREC_BF16X3;
         if (split && !kCfgs[dp.active].v2 && (!dp.ops_split || !dp.x_split))
                 return set_error(T3NS_E_ARG, "matvec: split precision is not set up on this plan");
-        if (precision != T3NS_PREC_FP64 && !split)
+        if (bf && (kCfgs[dp.active].v2 || !dp.ops_bf16 || !dp.x_bf16))
+                return set_error(T3NS_E_ARG, kCfgs[dp.active].v2
+                                                     ? "matvec: BF16x3 runs on configurations 0-2 only"
+                                                     : "matvec: BF16x3 is not set up on this plan");
+        if (precision != T3NS_PREC_FP64 && !split && !bf)
                 return set_error(T3NS_E_ARG, "matvec: unsupported precision");
         T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
         if (launches) *launches = 0;
         if (dt.n_units == 0) return T3NS_OK;
         // the contraction-ordered kernel splits the staged blocks itself
         if (split && !kCfgs[dp.active].v2) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
+        if (bf) T3NS_TRY(convert_to_bf16_pairs(x, dp.x_bf16, dp.size, s));
         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
         static_assert(kNumCfgs == 5, "one launch branch per configuration");
         int rc;
@@ -1799,6 +1988,12 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         } else if (dp.active == 4) {
                 rc = split ? launch_v2<CfgV2Large, true>(dp, dt, x, y, s)
                            : launch_v2<CfgV2Large, false>(dp, dt, x, y, s);
+        } else if (bf) {
+                const BfPair *xs = reinterpret_cast<const BfPair *>(dp.x_bf16);
+                const BfPair *os = reinterpret_cast<const BfPair *>(dp.ops_bf16);
+                rc = dp.active == 0   ? launch_cfg<CfgLarge, BfPair>(dp, dt, xs, os, y, s)
+                     : dp.active == 1 ? launch_cfg<CfgSmall, BfPair>(dp, dt, xs, os, y, s)
+                                      : launch_cfg<CfgWide, BfPair>(dp, dt, xs, os, y, s);
         } else if (split) {
                 const float2 *xs = dp.x_split, *os = dp.ops_split;
                 rc = dp.active == 0   ? launch_cfg<CfgLarge, float2>(dp, dt, xs, os, y, s)
@@ -1810,7 +2005,7 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
                                       : launch_cfg<CfgWide, double>(dp, dt, x, dp.ops, y, s);
         }
         T3NS_TRY(rc);
-        if (launches) *launches = (split && !kCfgs[dp.active].v2) ? 2 : 1;
+        if (launches) *launches = ((split && !kCfgs[dp.active].v2) || bf) ? 2 : 1;
         return T3NS_OK;
 }
 

@@ -74,14 +74,15 @@ int64_t estimate_solve_bytes(const t3ns_heff_desc *d, int precision, int max_vec
         for (int64_t c = 0; c < d->combo_ptr[npairs]; ++c)
                 tasks += d->MPOc_beg[d->combo_mpo[c] + 1] - d->MPOc_beg[d->combo_mpo[c]];
         const bool split = precision == T3NS_PREC_3XTF32;
-        int64_t b = op_elems * (split ? 16 : 8);               // FP64 (+ {hi, lo} pairs)
+        const bool bf = precision == T3NS_PREC_BF16X3;
+        int64_t b = op_elems * (split ? 16 : bf ? 12 : 8);     // FP64 (+ {hi, lo} pairs)
         // the transposed operators of the contraction-ordered configurations
         // (rows padded to 4: bounded here by twice the operators; their {hi, lo}
         // pairs too in split precision) and their offsets per term
         b += op_elems * (split ? 32 : 16) + tasks * 3 * (int64_t) sizeof(int64_t);
         b += tasks * (int64_t) sizeof(HeffTask);
         b += kNumCfgs * npairs * (int64_t) (sizeof(HeffPair) + 4 * sizeof(HeffUnit));
-        b += n * (16 + (split ? 8 : 0));                      // plan staging (+ split input)
+        b += n * (16 + (split ? 8 : bf ? 4 : 0));             // plan staging (+ split input)
         b += n * 8 * (2 * (int64_t) std::max(max_vecs, 3) + 6); // basis + work vectors
         return b + b / 20 + (16 << 20);                      // 5% + 16 MiB slack
 }

@@ -13,13 +13,14 @@ import pytest
 
 import oracle_lib
 from conftest import ROOT
-from t3ns_b200.native import T3NS_PREC_3XTF32, HeffPlan, StepDesc
+from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_BF16X3, HeffPlan, StepDesc
 from t3ns_b200.stepfile import read_step
 
 pytestmark = pytest.mark.gpu
 
 MATVEC_RTOL = 1e-12
 SPLIT_RTOL = 5e-6          # as tests/test_heff_gpu.py (3xTF32, FP32 accumulation)
+BF16_RTOL = 2e-4           # as tests/test_bf16x3.py (BF16x3, FP32 accumulation)
 
 D512 = os.path.join(ROOT, "oracle", "_ref", "captures", "qc24_D512", "step_006.t3c")
 WORKLOADS = sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "workloads", "*.t3c")))
@@ -74,6 +75,17 @@ def test_d512_split_precision_error(d512, config):
     plan.close()
 
 
+@pytest.mark.parametrize("config", [0, 1, 2])
+def test_d512_bf16x3_error(d512, config):
+    s, d = d512
+    plan = HeffPlan(d, T3NS_PREC_BF16X3)
+    plan.set_config(config)
+    for v in range(2):
+        err = _rel(plan.matvec_host(s[f"x{v}"]), s[f"y{v}"])
+        assert err <= BF16_RTOL, err
+    plan.close()
+
+
 @pytest.mark.parametrize("path", WORKLOADS, ids=os.path.basename)
 def test_workload_matches_oracle_on_sampled_blocks(path, cuda):
     s = read_step(path)
@@ -95,3 +107,7 @@ def test_workload_matches_oracle_on_sampled_blocks(path, cuda):
     err = _rel(split.matvec_host(x)[sel], yo[sel])
     split.close()
     assert err <= SPLIT_RTOL, err
+    bf = HeffPlan(d, T3NS_PREC_BF16X3)
+    err = _rel(bf.matvec_host(x)[sel], yo[sel])
+    bf.close()
+    assert err <= BF16_RTOL, err
