@@ -138,10 +138,13 @@ int t3ns_heff_diagonal_host(t3ns_heff *h, double *diag);
  * tiles, 2 = one 768-thread CTA per SM (more warps, fewer registers a thread)
  * with mid-size tiles; 3 and 4 = the contraction-ordered kernel (every stage
  * contracts the fastest axis of its input, operators transposed on the
- * device) with 768 and 512 threads, FP64 and 3xTF32.  Each has its own tiling
- * of the plan (built on first use).  A BF16x3 plan runs configurations 0-2
- * only (selecting 3 or 4 is an error, T3NS_E_ARG). */
-#define T3NS_NUM_CONFIGS 5
+ * device) with 768 and 512 threads, FP64 and 3xTF32; 5, 6, 7 = the shapes of
+ * 0, 1, 2 with buffers sized for BF16x3 (twice the elements in the same
+ * shared memory), BF16x3 only.  Each has its own tiling of the plan (built on
+ * first use).  Selecting a configuration that does not run the plan's
+ * precision is an error (T3NS_E_ARG); switching the precision falls back to
+ * configuration 0 when the active one does not run the new precision. */
+#define T3NS_NUM_CONFIGS 8
 int t3ns_heff_set_config(t3ns_heff *h, int config);
 int t3ns_heff_get_config(const t3ns_heff *h);
 

@@ -413,11 +413,17 @@ static void capture_structure(const struct Heffdata *hd, int size)
 
         static int (*wr)(const struct Heffdata *, const char *);
         if (!wr) {
-                void *h = opt_schedule_lib ? dlopen(opt_schedule_lib, RTLD_NOW | RTLD_LOCAL)
-                                           : RTLD_DEFAULT;
-                wr = h ? (int (*)(const struct Heffdata *, const char *))
-                                 dlsym(h, "t3ns_dropin_schedule_write")
-                       : NULL;
+                /* the drop-in build links the compiler; the oracle build loads
+                 * it privately from --schedule-lib (RTLD_DEFAULT is a null
+                 * handle, so the two cases are told apart by the option) */
+                if (opt_schedule_lib) {
+                        void *h = dlopen(opt_schedule_lib, RTLD_NOW | RTLD_LOCAL);
+                        if (h) wr = (int (*)(const struct Heffdata *, const char *))
+                                        dlsym(h, "t3ns_dropin_schedule_write");
+                } else {
+                        wr = (int (*)(const struct Heffdata *, const char *))
+                                dlsym(RTLD_DEFAULT, "t3ns_dropin_schedule_write");
+                }
                 if (!wr) { fprintf(stderr, "no t3ns_dropin_schedule_write\n"); exit(EXIT_FAILURE); }
         }
         char sp[4096];

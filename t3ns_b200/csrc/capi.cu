@@ -141,12 +141,13 @@ static int setup_precision(t3ns_heff *h, int precision)
             precision != T3NS_PREC_BF16X3)
                 return set_error(T3NS_E_ARG, "unknown precision");
         DevicePlan &dp = h->dp;
+        if (!cfg_supports(dp.active, precision)) {
+                // the active configuration does not run this precision
+                // (3, 4: not BF16x3; 5-7: BF16x3 only): fall back to 0
+                T3NS_TRY(upload_tiles(h, 0));
+                dp.active = 0;
+        }
         if (precision == T3NS_PREC_BF16X3) {
-                // BF16x3 runs on the configurations 0-2 (heff_kernel)
-                if (kCfgs[dp.active].v2) {
-                        T3NS_TRY(upload_tiles(h, 0));
-                        dp.active = 0;
-                }
                 if (!dp.ops_bf16) {
                         T3NS_TRY(dev_alloc(h, &dp.ops_bf16, (size_t) h->hp.op_elems));
                         T3NS_TRY(dev_alloc(h, &dp.x_bf16, (size_t) h->hp.size));
@@ -311,8 +312,10 @@ int t3ns_heff_set_config(t3ns_heff *h, int config)
 {
         if (!h) return set_error(T3NS_E_ARG, "null plan");
         if (config < 0 || config >= kNumCfgs) return set_error(T3NS_E_ARG, "unknown configuration");
-        if (h->precision == T3NS_PREC_BF16X3 && kCfgs[config].v2)
-                return set_error(T3NS_E_ARG, "BF16x3 runs on configurations 0-2 only");
+        if (!cfg_supports(config, h->precision))
+                return set_error(T3NS_E_ARG, "configuration " + std::to_string(config) +
+                                                     " does not run this precision "
+                                                     "(3, 4: FP64 and 3xTF32; 5-7: BF16x3)");
         T3NS_TRY(upload_tiles(h, config));
         h->dp.active = config;
         return T3NS_OK;
@@ -340,7 +343,7 @@ int t3ns_heff_autotune(t3ns_heff *h, int reps, int force, double *ms_out)
         int rc = T3NS_OK;
         bool first = true;
         for (int c = 0; c < kNumCfgs && rc == T3NS_OK; ++c) {
-                if (h->precision == T3NS_PREC_BF16X3 && kCfgs[c].v2) continue;
+                if (!cfg_supports(c, h->precision)) continue;
                 rc = t3ns_heff_set_config(h, c);
                 if (rc != T3NS_OK) break;
                 // one untimed run, then `reps` timed ones

@@ -78,6 +78,22 @@ struct CfgWide {
 // Contraction-ordered kernel (heff_v2.cuh): 768 threads with 6,144-element
 // output tiles, and 512 threads with 8,192; both stage old blocks of up to
 // 4,096 padded elements.
+// BF16x3 tilings of the three configurations above: an output tile of FP32
+// accumulators and BF16-pair intermediates take half the bytes of FP64
+// elements, so the same shared memory holds twice the elements (kOut here
+// in FP32 elements; kPsi and kW in FP64-sized slots, two BF16 pairs each).
+struct CfgLargeB {
+        static constexpr int kThreads = 512, kMinBlocks = 1;
+        static constexpr int kOut = 16384, kPsi = 1024, kW = 17408;
+};
+struct CfgSmallB {
+        static constexpr int kThreads = 256, kMinBlocks = 2;
+        static constexpr int kOut = 6144, kPsi = 1024, kW = 9472;
+};
+struct CfgWideB {
+        static constexpr int kThreads = 768, kMinBlocks = 1;
+        static constexpr int kOut = 12288, kPsi = 1024, kW = 19456;
+};
 struct CfgV2Wide {
         static constexpr int kThreads = 768, kMinBlocks = 1;
         static constexpr int kOut = 6144, kPsi = 4096, kW = 17408;
@@ -97,7 +113,22 @@ const KernelCfg kCfgs[kNumCfgs] = {
          "fp64-ordered-768x1-out6144", 1},
         {CfgV2Large::kThreads, CfgV2Large::kMinBlocks, CfgV2Large::kOut, CfgV2Large::kPsi,
          CfgV2Large::kW, "fp64-ordered-512x1-out8192", 1},
+        // BF16x3 only: plan capacities in BF16 pairs (twice the FP64 slots)
+        {CfgLargeB::kThreads, CfgLargeB::kMinBlocks, CfgLargeB::kOut, 2 * CfgLargeB::kPsi,
+         2 * CfgLargeB::kW, "bf16-512x1-out16384", 0, 1},
+        {CfgSmallB::kThreads, CfgSmallB::kMinBlocks, CfgSmallB::kOut, 2 * CfgSmallB::kPsi,
+         2 * CfgSmallB::kW, "bf16-256x2-out6144", 0, 1},
+        {CfgWideB::kThreads, CfgWideB::kMinBlocks, CfgWideB::kOut, 2 * CfgWideB::kPsi,
+         2 * CfgWideB::kW, "bf16-768x1-out12288", 0, 1},
 };
+
+bool cfg_supports(int cfg, int precision)
+{
+        if (cfg < 0 || cfg >= kNumCfgs) return false;
+        if (kCfgs[cfg].bf16) return precision == T3NS_PREC_BF16X3;
+        if (kCfgs[cfg].v2) return precision != T3NS_PREC_BF16X3;
+        return true;
+}
 
 
 // D(8x8) += A(8x4) * B(4x8) on the FP64 tensor pipe (one warp).  Fragment
@@ -1550,17 +1581,32 @@ int build_plan(const t3ns_heff_desc *d, HostPlan &hp)
                                 int dax = -1;
                                 double dfrac = 1.0;
                                 if (nops == 3) {
-                                        // the axis with the fewest distinct operator blocks;
-                                        // the pair's terms sorted by it (stable)
+                                        // the axis whose shared first stage gives the
+                                        // cheapest untiled sequence (distinct operator
+                                        // blocks / terms on it scale that stage); the
+                                        // pair's terms sorted by it (stable)
                                         std::vector<int64_t> v(t1 - t0);
+                                        const int eo[3] = {eo4.x, eo4.y, eo4.z};
+                                        const int en3[3] = {dn[hp.map[0]], dn[hp.map[1]], dn[hp.map[2]]};
+                                        const int nt1[3] = {1, 1, 1};
+                                        double best = 0;
                                         for (int ax = 0; ax < 3; ++ax) {
                                                 for (int t = t0; t < t1; ++t) v[t - t0] = hp.tasks[t].op_off[ax];
                                                 std::sort(v.begin(), v.end());
-                                                const double nd = (double) (std::unique(v.begin(), v.end()) -
-                                                                            v.begin());
-                                                if (dax < 0 || nd / (t1 - t0) < dfrac) {
+                                                const double fr = (double) (std::unique(v.begin(), v.end()) -
+                                                                            v.begin()) / (t1 - t0);
+                                                double cost = 0;
+                                                for (int q = 0; q < 6; ++q) {
+                                                        const int *sq = kOrders3[q];
+                                                        int64_t s1, s2;
+                                                        const double c = seq_cost(sq, 3, eo, en3, en3, nt1, &s1, &s2,
+                                                                                  sq[0] == ax ? fr : 1.0);
+                                                        if (q == 0 || c < cost) cost = c;
+                                                }
+                                                if (dax < 0 || cost < best) {
                                                         dax = ax;
-                                                        dfrac = nd / (t1 - t0);
+                                                        dfrac = fr;
+                                                        best = cost;
                                                 }
                                         }
                                         std::stable_sort(hp.tasks.begin() + t0, hp.tasks.begin() + t1,
@@ -1936,7 +1982,7 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
                 // the same kernel, one launch per output block (its own unit run)
                 const DeviceTiles &full = dp.tiles[dp.active];
                 if (!full.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
-                if (precision != T3NS_PREC_FP64)
+                if (precision != T3NS_PREC_FP64 || !cfg_supports(dp.active, precision))
                         return set_error(T3NS_E_ARG, "matvec: per-block dispatch is FP64 only");
                 T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
                 DevicePlan one = dp;
@@ -1967,10 +2013,11 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         const bool bf = precision == T3NS_PREC_BF16X3;
         if (split && !kCfgs[dp.active].v2 && (!dp.ops_split || !dp.x_split))
                 return set_error(T3NS_E_ARG, "matvec: split precision is not set up on this plan");
-        if (bf && (kCfgs[dp.active].v2 || !dp.ops_bf16 || !dp.x_bf16))
-                return set_error(T3NS_E_ARG, kCfgs[dp.active].v2
-                                                     ? "matvec: BF16x3 runs on configurations 0-2 only"
-                                                     : "matvec: BF16x3 is not set up on this plan");
+        if (!cfg_supports(dp.active, precision))
+                return set_error(T3NS_E_ARG, "matvec: configuration " + std::to_string(dp.active) +
+                                                     " does not run this precision");
+        if (bf && (!dp.ops_bf16 || !dp.x_bf16))
+                return set_error(T3NS_E_ARG, "matvec: BF16x3 is not set up on this plan");
         if (precision != T3NS_PREC_FP64 && !split && !bf)
                 return set_error(T3NS_E_ARG, "matvec: unsupported precision");
         T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
@@ -1980,7 +2027,7 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         if (split && !kCfgs[dp.active].v2) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
         if (bf) T3NS_TRY(convert_to_bf16_pairs(x, dp.x_bf16, dp.size, s));
         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
-        static_assert(kNumCfgs == 5, "one launch branch per configuration");
+        static_assert(kNumCfgs == 8, "one launch branch per configuration");
         int rc;
         if (dp.active == 3) {
                 rc = split ? launch_v2<CfgV2Wide, true>(dp, dt, x, y, s)
@@ -1991,9 +2038,14 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         } else if (bf) {
                 const BfPair *xs = reinterpret_cast<const BfPair *>(dp.x_bf16);
                 const BfPair *os = reinterpret_cast<const BfPair *>(dp.ops_bf16);
-                rc = dp.active == 0   ? launch_cfg<CfgLarge, BfPair>(dp, dt, xs, os, y, s)
-                     : dp.active == 1 ? launch_cfg<CfgSmall, BfPair>(dp, dt, xs, os, y, s)
-                                      : launch_cfg<CfgWide, BfPair>(dp, dt, xs, os, y, s);
+                switch (dp.active) {
+                case 0: rc = launch_cfg<CfgLarge, BfPair>(dp, dt, xs, os, y, s); break;
+                case 1: rc = launch_cfg<CfgSmall, BfPair>(dp, dt, xs, os, y, s); break;
+                case 2: rc = launch_cfg<CfgWide, BfPair>(dp, dt, xs, os, y, s); break;
+                case 5: rc = launch_cfg<CfgLargeB, BfPair>(dp, dt, xs, os, y, s); break;
+                case 6: rc = launch_cfg<CfgSmallB, BfPair>(dp, dt, xs, os, y, s); break;
+                default: rc = launch_cfg<CfgWideB, BfPair>(dp, dt, xs, os, y, s); break;
+                }
         } else if (split) {
                 const float2 *xs = dp.x_split, *os = dp.ops_split;
                 rc = dp.active == 0   ? launch_cfg<CfgLarge, float2>(dp, dt, xs, os, y, s)

@@ -52,9 +52,14 @@ struct KernelCfg {
         int w_cap;         // intermediates of a group of terms
         const char *name;
         int v2;            // 1: contraction-ordered layouts (heff_v2_kernel)
+        int bf16;          // 1: BF16x3 only, buffers sized in BF16 pairs
 };
-constexpr int kNumCfgs = 5;
-constexpr int kV2First = 3;   // configurations kV2First.. run heff_v2_kernel
+constexpr int kNumCfgs = 8;
+constexpr int kV2First = 3;   // configurations 3, 4 run heff_v2_kernel
+constexpr int kBfFirst = 5;   // configurations 5-7: BF16x3 tilings of 0-2
+
+// Whether configuration cfg runs matvecs in arithmetic `precision`.
+bool cfg_supports(int cfg, int precision);
 extern const KernelCfg kCfgs[kNumCfgs];
 
 // One (new, old) pair before tiling: its terms and the old block's dims.

@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(_HERE, "_lib")
 
 T3NS_PREC_FP64 = 0
-T3NS_NUM_CONFIGS = 5   # kernel configurations of the matvec (3, 4: FP64 only)
+T3NS_NUM_CONFIGS = 8   # kernel configurations (3, 4: not BF16x3; 5-7: BF16x3 only)
 T3NS_PREC_3XTF32 = 1
 T3NS_PREC_BF16X3 = 2
 
@@ -255,7 +255,7 @@ class HeffPlan:
     def autotune(self, reps: int = 2, force: bool = True):
         """Time every kernel configuration and keep the fastest; returns the
         median milliseconds per configuration (0 where not timed)."""
-        ms = (C.c_double * 8)()
+        ms = (C.c_double * 16)()
         check(self.lib.t3ns_heff_autotune(self.h, reps, int(force), ms), "autotune")
         return [ms[i] for i in range(T3NS_NUM_CONFIGS)]
 

@@ -34,7 +34,7 @@ def torch_cuda():
     return torch
 
 
-@pytest.mark.parametrize("config", [0, 1, 2])
+@pytest.mark.parametrize("config", [0, 1, 2, 5, 6, 7])
 @pytest.mark.parametrize("path", STEPS[::2], ids=lambda p: "/".join(p.split("/")[-2:]))
 def test_bf16x3_matvec_error(path, config, torch_cuda):
     s = read_step(path)
@@ -48,17 +48,24 @@ def test_bf16x3_matvec_error(path, config, torch_cuda):
     plan.close()
 
 
-def test_bf16x3_rejects_contraction_ordered_configs(torch_cuda):
+def test_configs_reject_other_precisions(torch_cuda):
+    """3 and 4 do not run BF16x3, 5-7 run only BF16x3; switching the
+    precision falls back to configuration 0 from one that does not run it."""
     s = read_step(golden_steps()[0])
     plan = HeffPlan(StepDesc(s), T3NS_PREC_BF16X3)
     for c in (3, 4):
         with pytest.raises(RuntimeError):
             plan.set_config(c)
-    # switching precision keeps the plan usable in both
-    plan.set_precision(T3NS_PREC_FP64)
+    plan.set_config(5)
+    assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= BF16_RTOL
+    plan.set_precision(T3NS_PREC_FP64)      # 5 is BF16x3 only
+    assert plan.config() == 0
+    for c in (5, 6, 7):
+        with pytest.raises(RuntimeError):
+            plan.set_config(c)
     plan.set_config(3)
     assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= 1e-12
-    plan.set_precision(T3NS_PREC_BF16X3)   # falls back to configuration 0
+    plan.set_precision(T3NS_PREC_BF16X3)   # 3 does not run BF16x3
     assert plan.config() == 0
     assert _rel(plan.matvec_host(s["x0"]), s["y0"]) <= BF16_RTOL
     plan.close()

@@ -75,7 +75,7 @@ def test_d512_split_precision_error(d512, config):
     plan.close()
 
 
-@pytest.mark.parametrize("config", [0, 1, 2])
+@pytest.mark.parametrize("config", [0, 1, 2, 5, 6, 7])
 def test_d512_bf16x3_error(d512, config):
     s, d = d512
     plan = HeffPlan(d, T3NS_PREC_BF16X3)
@@ -108,6 +108,8 @@ def test_workload_matches_oracle_on_sampled_blocks(path, cuda):
     split.close()
     assert err <= SPLIT_RTOL, err
     bf = HeffPlan(d, T3NS_PREC_BF16X3)
-    err = _rel(bf.matvec_host(x)[sel], yo[sel])
+    for config in (0, 5, 7):
+        bf.set_config(config)
+        err = _rel(bf.matvec_host(x)[sel], yo[sel])
+        assert err <= BF16_RTOL, (config, err)
     bf.close()
-    assert err <= BF16_RTOL, err

@@ -21,7 +21,9 @@ def _check(s, plan, blocks):
     assert fl[1] >= pe.shared_flops_lower_bound(plan) * (1 - 1e-12)
 
 
-CONFIGS = (0, 1, 2, 3, 4)   # the engine's kernel configurations (3, 4: contraction-ordered)
+# the engine's kernel configurations (3, 4: contraction-ordered; 5, 7: BF16x3
+# tilings with twice the elements per buffer)
+CONFIGS = (0, 1, 2, 3, 4, 5, 7)
 
 
 @pytest.mark.parametrize("config", CONFIGS)
@@ -45,7 +47,7 @@ def test_plan_emulation_tiled_and_split_blocks(config):
     e = plan["plan.edims"].reshape(-1, 3)
     tiled = (u[:, 2] < e[u[:, 0], 1]) | (u[:, 4] < e[u[:, 0], 2]) | (u[:, 6] < e[u[:, 0], 0])
     split = u[:, 9] != 0
-    if config == 0 and not tiled.any():
+    if config in (0, 5, 7) and not tiled.any():
         tiled = split
     assert tiled.any()
     blocks = sorted({int(u[np.nonzero(tiled)[0][0], 0])} |
