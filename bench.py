@@ -220,13 +220,13 @@ def run_engine(args, rank, world):
     from t3ns_b200.native import T3NS_PREC_3XTF32, T3NS_PREC_BF16X3, T3NS_PREC_FP64
     y64 = y.clone()
 
-    def time_precision(prec):
+    def time_precision(prec, fixed_config):
         plan.set_precision(prec)
-        if args.split_kernel_config is None:
+        if fixed_config is None:
             tune = plan.autotune(reps=1)
         else:
             tune = None
-            plan.set_config(args.split_kernel_config)
+            plan.set_config(fixed_config)
         for _ in range(args.warmup):
             plan.matvec_device(x.data_ptr(), y.data_ptr(), sh)
         torch.cuda.synchronize()
@@ -243,8 +243,9 @@ def run_engine(args, rank, world):
         t = float(sum(a.elapsed_time(b) * 1e-3 for a, b in ts))
         return t, float((y - y64).norm() / y64.norm()), plan.config(), tune
 
-    t_split, split_err, split_cfg, split_tune = time_precision(T3NS_PREC_3XTF32)
-    t_bf, bf_err, bf_cfg, bf_tune = time_precision(T3NS_PREC_BF16X3)
+    t_split, split_err, split_cfg, split_tune = time_precision(T3NS_PREC_3XTF32,
+                                                              args.split_kernel_config)
+    t_bf, bf_err, bf_cfg, bf_tune = time_precision(T3NS_PREC_BF16X3, args.bf16_kernel_config)
     plan.set_precision(T3NS_PREC_FP64)
     if args.kernel_config is None:
         plan.autotune(reps=1, force=False)
@@ -337,7 +338,7 @@ def sweep_comparison(timeout=900):
     out = {}
     for name, args in cases.items():
         rec = {}
-        for prec in ("fp64", "3xtf32"):
+        for prec in ("fp64", "3xtf32", "bf16x3"):
             env = dict(os.environ, T3NS_B200_PRECISION=prec, OMP_NUM_THREADS="8",
                        OPENBLAS_NUM_THREADS="1")
             r = subprocess.run([exe, *args, "--init", "c"], capture_output=True, text=True,
@@ -351,6 +352,8 @@ def sweep_comparison(timeout=900):
             f["timers"].get("Heff T3NS: matvec", 0) + f["timers"].get("Heff DMRG: matvec", 0)) / max(
             m["timers"].get("Heff T3NS: matvec", 0) + m["timers"].get("Heff DMRG: matvec", 0), 1e-12)
         rec["abs_dE_mixed_vs_fp64"] = abs(m["energy"] - f["energy"])
+        rec["speedup_bf16x3_vs_fp64"] = f["sweep_seconds"] / rec["bf16x3"]["sweep_seconds"]
+        rec["abs_dE_bf16x3_vs_fp64"] = abs(rec["bf16x3"]["energy"] - f["energy"])
         out[name] = rec
     out["note"] = ("timers are the reference's own buckets over the whole scheme "
                    "(src/optimize_network.c:43-95): 'Heff ...: matvec' is the Davidson solves, "
@@ -393,7 +396,8 @@ def davidson_comparison(path=None, max_its=100, seed=7):
     path = path or os.path.join(ROOT, "oracle", "_ref", "captures", "qc24_D512", "step_006.t3c")
     if not os.path.exists(path):
         return None
-    from t3ns_b200.native import HeffPlan, StepDesc, T3NS_PREC_3XTF32, T3NS_PREC_FP64
+    from t3ns_b200.native import (HeffPlan, StepDesc, T3NS_PREC_3XTF32, T3NS_PREC_BF16X3,
+                                  T3NS_PREC_FP64)
     from t3ns_b200.stepfile import read_step
     s = read_step(path)
     desc = StepDesc(s)
@@ -406,7 +410,8 @@ def davidson_comparison(path=None, max_its=100, seed=7):
            "max_its": max_its,
            "guess": "FP64 solve from seeded N(0,1) to residual %.1e (%d iterations)"
                     % (pinfo["residual"], pinfo["iterations"])}
-    for name, prec in (("fp64", T3NS_PREC_FP64), ("3xtf32", T3NS_PREC_3XTF32)):
+    for name, prec in (("fp64", T3NS_PREC_FP64), ("3xtf32", T3NS_PREC_3XTF32),
+                       ("bf16x3", T3NS_PREC_BF16X3)):
         plan = HeffPlan(desc, prec)
         plan.autotune(reps=1, force=False)
         g = g0.copy()
@@ -418,6 +423,8 @@ def davidson_comparison(path=None, max_its=100, seed=7):
         plan.close()
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["3xtf32"]["seconds"]
     out["abs_dE_mixed_vs_fp64"] = abs(out["3xtf32"]["energy"] - out["fp64"]["energy"])
+    out["speedup_bf16x3_vs_fp64"] = out["fp64"]["seconds"] / out["bf16x3"]["seconds"]
+    out["abs_dE_bf16x3_vs_fp64"] = abs(out["bf16x3"]["energy"] - out["fp64"]["energy"])
     return out
 
 
@@ -681,7 +688,9 @@ def main():
                          "autotuner's choice (profiling: the autotuner's event timing is "
                          "distorted under a profiler)")
     ap.add_argument("--split-kernel-config", type=int, default=None,
-                    help="the same for the split-precision matvec")
+                    help="the same for the 3xTF32 matvec")
+    ap.add_argument("--bf16-kernel-config", type=int, default=None,
+                    help="the same for the BF16x3 matvec")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true",
                     help="skip the whole-sweep FP64 vs split-precision comparison")

@@ -22,6 +22,7 @@
 // to a per-CTA scratch slice, the second accumulates into the output; both
 // run on the FP64 tensor pipe (cta_dgemm).
 #include <algorithm>
+#include <numeric>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -142,11 +143,18 @@ bupdate_kernel(int3 ax, int nunits, const int *__restrict__ unit_ptr,
                         const int x1 = a_first ? a : b, x2 = a_first ? b : a;
                         int v1[3] = {kd[0], kd[1], kd[2]};
                         v1[x1] = bd[x1];
+                        // the host orders an entry's triples by their first-applied
+                        // operator: a first stage equal to the previous one is reused
+                        // (W1 is written by the first stage only)
+                        const double *prev = nullptr;
                         for (int p = op_ptr[e]; p < op_ptr[e + 1]; ++p) {
                                 const double *P1 = a_first ? O1 + o1_off[p] : O2 + o2_off[p];
                                 const double *P2 = a_first ? O2 + o2_off[p] : O1 + o1_off[p];
-                                apply_axis_dmma(x1, kd, bd[x1], P1, Tk, W1);
-                                __syncthreads();
+                                if (P1 != prev) {
+                                        apply_axis_dmma(x1, kd, bd[x1], P1, Tk, W1);
+                                        __syncthreads();
+                                        prev = P1;
+                                }
                                 apply_axis_dmma(x2, v1, bd[x2], P2, W1, W2);
                                 __syncthreads();
                                 double *Nw = NEW + new_off[p];
@@ -602,9 +610,33 @@ int bupdate_run(const t3ns_bupdate_desc *d, const double *t_tel, const double *o
         const size_t o_t = L.input(d->t_off, d->nentries);
         const size_t o_ta = L.input(d->ta_off, d->nentries);
         const size_t o_pref = L.input(d->pref, d->nentries);
-        const size_t o_o1_off = L.input(d->o1_off, ntr);
-        const size_t o_o2_off = L.input(d->o2_off, ntr);
-        const size_t o_new_off = L.input(d->new_off, ntr);
+        // each entry's triples ordered by the operator the kernel applies
+        // first (the same order choice as the kernel's), so equal first
+        // stages run once; the triples of an entry write their own new
+        // blocks, so only the summation order into a shared block changes
+        std::vector<int64_t> s_o1(ntr), s_o2(ntr), s_new(ntr);
+        {
+                std::vector<int> idx;
+                for (int e = 0; e < d->nentries; ++e) {
+                        const int *kd = d->dims + 6 * e, *bd = kd + 3;
+                        const bool a_first = (int64_t) kd[b] * bd[a] * (kd[a] + bd[b]) <=
+                                             (int64_t) kd[a] * bd[b] * (kd[b] + bd[a]);
+                        const int p0 = d->op_ptr[e], p1 = d->op_ptr[e + 1];
+                        idx.resize(p1 - p0);
+                        std::iota(idx.begin(), idx.end(), p0);
+                        const int64_t *key = a_first ? d->o1_off : d->o2_off;
+                        std::stable_sort(idx.begin(), idx.end(),
+                                         [key](int x, int y) { return key[x] < key[y]; });
+                        for (int q = p0; q < p1; ++q) {
+                                s_o1[q] = d->o1_off[idx[q - p0]];
+                                s_o2[q] = d->o2_off[idx[q - p0]];
+                                s_new[q] = d->new_off[idx[q - p0]];
+                        }
+                }
+        }
+        const size_t o_o1_off = L.input(s_o1.data(), ntr);
+        const size_t o_o2_off = L.input(s_o2.data(), ntr);
+        const size_t o_new_off = L.input(s_new.data(), ntr);
         const size_t o_T = L.input(t_tel, d->t_elems);
         const size_t o_O1 = L.input(o1_tel, d->o1_elems);
         const size_t o_O2 = L.input(o2_tel, d->o2_elems);
