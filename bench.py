@@ -363,6 +363,42 @@ def sweep_comparison(timeout=900):
     return out
 
 
+def sweep_qc24(D, precisions=("fp64", "bf16x3", "3xtf32"), timeout=3000):
+    """One whole sweep (SITE_SIZE 2) of the reference driver linked against
+    the drop-in on the 24-orbital synthetic QC Hamiltonian at bond dimension
+    D, once per arithmetic mode: sweep seconds, the reference's own timer
+    buckets, Davidson iteration counts, final energies and their differences
+    from the FP64 run.  Run on request (--sweep-qc24 D): at D=512 one FP64
+    sweep takes tens of minutes on one GPU."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "t3ns_run_dropin")
+    if not os.path.exists(exe):
+        return None
+    from t3ns_b200.workloads import synthetic_qc_fcidump
+    tmp = tempfile.mkdtemp(prefix="t3ns_bench_")
+    fcid = synthetic_qc_fcidump(os.path.join(tmp, "qc24.FCIDUMP"), 24, 24, 0, 72)
+    args = ["--net", os.path.join(ROOT, "tests", "golden", "networks", "t3ns_24.netw"),
+            "--inter", fcid, "--symm", "Z2,U1,SU2", "--ts", "0,24,0",
+            "--regime", f"{D},{D},0,2,1e-5,100,1,1e-8,0", "--init", "c"]
+    out = {"D": D, "sweeps": 1, "site_size": 2}
+    for prec in precisions:
+        env = dict(os.environ, T3NS_B200_PRECISION=prec, OMP_NUM_THREADS="16",
+                   OPENBLAS_NUM_THREADS="1")
+        r = subprocess.run([exe, *args], capture_output=True, text=True, env=env, timeout=timeout)
+        if r.returncode != 0:
+            out[prec] = {"error": f"exit {r.returncode}"}
+            continue
+        rec = parse_sweep_run(r.stdout)
+        rec["init_seconds"] = float(re.findall(r"INIT_SECONDS (\S+)", r.stdout)[-1])
+        out[prec] = rec
+    f = out.get("fp64", {})
+    for prec in precisions[1:]:
+        m = out.get(prec, {})
+        if "sweep_seconds" in f and "sweep_seconds" in m:
+            out[f"speedup_{prec}_vs_fp64"] = f["sweep_seconds"] / m["sweep_seconds"]
+            out[f"abs_dE_{prec}_vs_fp64"] = abs(m["energy"] - f["energy"])
+    return out
+
+
 _TIMER = re.compile(r"^ \* (.+?)\s+:: ([0-9.]+) sec", re.M)
 
 
@@ -529,6 +565,12 @@ def other_rows_measurement(reps=3):
     return out
 
 
+# request sources of the serving measurement: the captured small steps and
+# the golden steps (each carries its reference Davidson energy)
+REQUEST_SOURCES = [os.path.join(ROOT, "oracle", "_ref", "captures", "*", "step_*.t3c"),
+                   os.path.join(ROOT, "tests", "golden", "*.t3c")]
+
+
 def serving_stream():
     """The engine's request loop under a Poisson stream of 128 independent
     ground-state solves (mean 4 arrivals/s; solves drawn from the captured
@@ -536,7 +578,7 @@ def serving_stream():
     admission budget, 4 in flight, split precision with FP64 defect
     correction: p50/p99 latency and solves/s."""
     from t3ns_b200.serving import Workload, request_steps, run_stream
-    steps = [p for p in request_steps() if "eig.energy" in Workload(p).step]
+    steps = request_steps(REQUEST_SOURCES)
     if not steps:
         return None
     _, summary = run_stream([Workload(p) for p in steps], n_requests=128, rate=4.0,
@@ -698,6 +740,9 @@ def main():
                     help="skip the request-stream (serving) measurement")
     ap.add_argument("--no-micro", action="store_true",
                     help="skip the three-site D=1024 matvec microbenchmark")
+    ap.add_argument("--sweep-qc24", type=int, default=None, metavar="D",
+                    help="also run one whole sweep of the 24-orbital QC Hamiltonian at bond "
+                         "dimension D through the drop-in in each arithmetic mode (long)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -773,6 +818,8 @@ def main():
             out["serving"] = serving_stream()
         if not args.no_sweep:
             out["updates_and_decomposition"] = other_rows_measurement()
+        if args.sweep_qc24:
+            out["sweep_qc24"] = sweep_qc24(args.sweep_qc24)
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

@@ -9,6 +9,11 @@ minutes on 8 cores: the initial renormalised operators dominate) and writes
 the structure-only benchmark workloads of steps 5 and 6.  Outputs go to
 oracle/_ref/ (git-ignored).
 
+``ensure_d1024_s3()`` captures the three-site D=1024 microbenchmark steps
+with the reference on the CPU (hours on 8 cores); ``d1024_s3_on_gpu()``
+builds the same steps' structure with the drop-in driver on a GPU machine
+(``python -m oracle.captures d1024-gpu``, minutes).
+
 ``trim(path)`` rewrites a captured step file keeping only the operator
 blocks that the step's schedule references (every other block is marked
 empty, its elements dropped).  The matvec, its diagonal and the reference's
@@ -254,9 +259,49 @@ def ensure_d1024_s3(threads=None):
                 structure_only(os.path.join(d, f), out, compress=True)
 
 
+def d1024_s3_on_gpu(outdir, threads=16, timeout=1700, limit=2):
+    """The same three-site D=1024 steps, built on a GPU machine: the drop-in
+    driver (oracle/_ref/t3ns_run_dropin) builds the initial operators and
+    runs the updates and decompositions on the GPU (about five minutes for
+    the initial operators, eleven to reach the second step: steps 3 and 5,
+    2,661 and 3,420 blocks) and, with --capture-structure, writes each
+    selected step's structure and the product's schedule for it without
+    solving it; the pairs are joined into compressed structure-only
+    workloads in outdir (about 1 and 2.3 GB: their schedules hold tens of
+    millions of terms, too large to travel, so they are built where they
+    are used).  Returns the workload paths."""
+    import glob
+    import subprocess
+    import tempfile
+    exe = os.path.join(REF, "t3ns_run_dropin")
+    tmp = tempfile.mkdtemp(prefix="t3ns_d1024_")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1",
+               T3NS_B200_AUTOTUNE="0")
+    with open(os.path.join(tmp, "run.log"), "w") as log:
+        subprocess.run([exe, "--net", os.path.join(NETS, "t3ns_24.netw"), "--inter", _fcidump(24),
+                        "--symm", "Z2,U1,SU2", "--ts", "0,24,0",
+                        "--regime", "1024,1024,0,3,1e-5,100,1,1e-8,0", "--init", "c",
+                        "--capture-structure", tmp, "--capture-min", "4000000",
+                        "--capture-max", "18000000", "--capture-limit", str(limit),
+                        "--capture-stop"],
+                       env=env, stdout=log, stderr=subprocess.STDOUT, timeout=timeout)
+    os.makedirs(outdir, exist_ok=True)
+    out = []
+    for t in sorted(glob.glob(os.path.join(tmp, "step_*.t3c"))):
+        sched = t.replace(".t3c", ".sched")
+        if os.path.exists(sched):
+            o = os.path.join(outdir, "qc24_D1024_s3_" + os.path.basename(t).replace("_", ""))
+            structure_from_capture(t, sched, o, compress=True)
+            out.append(o)
+    return out
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "d1024":
         ensure_d1024_s3()
+        sys.exit(0)
+    if sys.argv[1] == "d1024-gpu":
+        print(d1024_s3_on_gpu(os.path.join(REF, "workloads")))
         sys.exit(0)
     if sys.argv[1] == "small":
         ensure_small()

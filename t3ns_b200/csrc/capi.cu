@@ -149,10 +149,29 @@ static int setup_precision(t3ns_heff *h, int precision)
         }
         if (precision == T3NS_PREC_BF16X3) {
                 if (!dp.ops_bf16) {
-                        T3NS_TRY(dev_alloc(h, &dp.ops_bf16, (size_t) h->hp.op_elems));
-                        T3NS_TRY(dev_alloc(h, &dp.x_bf16, (size_t) h->hp.size));
-                        T3NS_TRY(convert_to_bf16_pairs(dp.ops, dp.ops_bf16, h->hp.op_elems, h->stream));
-                        T3NS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+                        const HostPlan &hp = h->hp;
+                        T3NS_TRY(dev_alloc(h, &dp.ops_bf16, 2 * (size_t) std::max<int64_t>(hp.op_elems, 1)));
+                        T3NS_TRY(dev_alloc(h, &dp.x_bf16, (size_t) hp.size));
+                        if (!hp.tjobs.empty()) {
+                                int64_t *d_jobs = nullptr;
+                                T3NS_CUDA_TRY(cudaMalloc(&d_jobs, sizeof(int64_t) * hp.tjobs.size()));
+                                const cudaError_t e = cudaMemcpy(d_jobs, hp.tjobs.data(),
+                                                                 sizeof(int64_t) * hp.tjobs.size(),
+                                                                 cudaMemcpyHostToDevice);
+                                int rc = e == cudaSuccess
+                                                 ? build_paired_bf16_ops(hp, dp, d_jobs, h->stream)
+                                                 : set_error(T3NS_E_CUDA, std::string("paired operators: upload: ") +
+                                                                                  cudaGetErrorString(e));
+                                if (rc == T3NS_OK) {
+                                        const cudaError_t se = cudaStreamSynchronize(h->stream);
+                                        if (se != cudaSuccess)
+                                                rc = set_error(T3NS_E_CUDA, std::string("paired operators: kernel: ") +
+                                                                                    cudaGetErrorString(se));
+                                }
+                                if (rc == T3NS_OK) rc = check_device_error(h);
+                                cudaFree(d_jobs);
+                                T3NS_TRY(rc);
+                        }
                 }
         }
         if (precision == T3NS_PREC_3XTF32 && !dp.ops_split) {

@@ -691,6 +691,114 @@ __device__ __forceinline__ void warp_tile_x3(float (&d)[RM][RN][4], const BfPair
         }
 }
 
+// The BF16x3 tile with the operator side in the k-paired layout of the
+// BF16 operator copy: element (r, k) of an operator block with leading
+// dimension ld (the new dim) at (k/2)*2*ld + 2*r + (k%2), an odd K padded
+// with a zero column, so the two K-consecutive pairs a lane needs come in
+// one 8-byte load.  A_PK / B_PK: which operand is the operator (unit row or
+// column stride there, k stride ak / bk = ld); the other is read as in
+// warp_tile_x3.  Every paired offset is even (the copy places a block at
+// twice its FP64 offset), so the 8-byte loads are aligned.
+template <int RM, int RN, bool A_PK, bool B_PK>
+__device__ __forceinline__ void warp_tile_x3_pk(float (&d)[RM][RN][4], const BfPair *Ab, int am,
+                                                int ak, const BfPair *Bb, int bk, int bn,
+                                                const RowSplit &rs, bool split_a, int K, int M,
+                                                int N, int m0, int n0, int g, int t)
+{
+        int ao[RM][2], bo[RN];
+#pragma unroll
+        for (int i = 0; i < RM; ++i)
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                        const int m = m0 + 16 * i + 8 * r + g;
+                        if (A_PK)
+                                ao[i][r] = m < M ? 2 * m + 2 * t * ak : -1;
+                        else
+                                ao[i][r] = m < M ? (int) (split_a ? rs.a_off(m) : (int64_t) m * am) +
+                                                           2 * t * ak
+                                                 : -1;
+                }
+#pragma unroll
+        for (int j = 0; j < RN; ++j) {
+                const int n = n0 + 8 * j + g;
+                if (B_PK)
+                        bo[j] = n < N ? 2 * n + 2 * t * bk : -1;
+                else
+                        bo[j] = n < N ? (int) (split_a ? (int64_t) n * bn : rs.a_off(n)) + 2 * t * bk : -1;
+        }
+        const uint32_t *A = reinterpret_cast<const uint32_t *>(Ab);
+        const uint32_t *B = reinterpret_cast<const uint32_t *>(Bb);
+        for (int k0 = 0, ka = 0, kb = 0; k0 < K; k0 += 16, ka += 16 * ak, kb += 16 * bk) {
+                const int kk = k0 + 2 * t;
+                const bool q0 = kk < K, q1 = kk + 1 < K, q2 = kk + 8 < K, q3 = kk + 9 < K;
+                uint32_t ah[RM][4], al[RM][4], bh[RN][2], bl[RN][2];
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int r = 0; r < 2; ++r) {
+                                const bool ok = ao[i][r] >= 0;
+                                const int o = ao[i][r] + ka;
+                                uint32_t e0 = 0u, e1 = 0u, e2 = 0u, e3 = 0u;
+                                if (A_PK) {
+                                        if (ok && q0) {
+                                                const uint2 v = *reinterpret_cast<const uint2 *>(A + o);
+                                                e0 = v.x;
+                                                e1 = v.y;
+                                        }
+                                        if (ok && q2) {
+                                                const uint2 v = *reinterpret_cast<const uint2 *>(A + o + 8 * ak);
+                                                e2 = v.x;
+                                                e3 = v.y;
+                                        }
+                                } else {
+                                        e0 = (ok && q0) ? A[o] : 0u;
+                                        e1 = (ok && q1) ? A[o + ak] : 0u;
+                                        e2 = (ok && q2) ? A[o + 8 * ak] : 0u;
+                                        e3 = (ok && q3) ? A[o + 9 * ak] : 0u;
+                                }
+                                ah[i][r] = pick(e0, e1, 0x5410);
+                                al[i][r] = pick(e0, e1, 0x7632);
+                                ah[i][r + 2] = pick(e2, e3, 0x5410);
+                                al[i][r + 2] = pick(e2, e3, 0x7632);
+                        }
+#pragma unroll
+                for (int j = 0; j < RN; ++j) {
+                        const bool ok = bo[j] >= 0;
+                        const int o = bo[j] + kb;
+                        uint32_t f0 = 0u, f1 = 0u, f2 = 0u, f3 = 0u;
+                        if (B_PK) {
+                                if (ok && q0) {
+                                        const uint2 v = *reinterpret_cast<const uint2 *>(B + o);
+                                        f0 = v.x;
+                                        f1 = v.y;
+                                }
+                                if (ok && q2) {
+                                        const uint2 v = *reinterpret_cast<const uint2 *>(B + o + 8 * bk);
+                                        f2 = v.x;
+                                        f3 = v.y;
+                                }
+                        } else {
+                                f0 = (ok && q0) ? B[o] : 0u;
+                                f1 = (ok && q1) ? B[o + bk] : 0u;
+                                f2 = (ok && q2) ? B[o + 8 * bk] : 0u;
+                                f3 = (ok && q3) ? B[o + 9 * bk] : 0u;
+                        }
+                        bh[j][0] = pick(f0, f1, 0x5410);
+                        bl[j][0] = pick(f0, f1, 0x7632);
+                        bh[j][1] = pick(f2, f3, 0x5410);
+                        bl[j][1] = pick(f2, f3, 0x7632);
+                }
+#pragma unroll
+                for (int i = 0; i < RM; ++i)
+#pragma unroll
+                        for (int j = 0; j < RN; ++j) {
+                                mma_bf16(d[i][j], al[i], bh[j]);
+                                mma_bf16(d[i][j], ah[i], bl[j]);
+                                mma_bf16(d[i][j], ah[i], bh[j]);
+                        }
+        }
+}
+
 // the 3xTF32 tile under the common name of the split stages
 template <int RM, int RN>
 __device__ __forceinline__ void warp_tile_x3(float (&d)[RM][RN][4], const float2 *Ab, int am,
@@ -776,16 +884,39 @@ __device__ __forceinline__ void grouped_stage_x_t(int ax, const int *w, int rows
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) d[i][j][q] = 0.f;
                 for (int gg = g0; gg < g1; gg += gstep) {
-                        const E *op = ops + opoff[gg];
                         const E *tin = in + (!ACC && in_idx ? in_idx[gg] : gg) * in_gs;
-                        const E *Ab = ax == 0 ? op : tin;
-                        const E *Bb = ax == 0 ? tin : op;
-                        if (swap)
-                                warp_tile_x3<RM, RN>(d, Bb, bn, bk, Ab, ak, 1, rs, false, K, Mt, Nt,
-                                                     m0, n0, g, t);
-                        else
-                                warp_tile_x3<RM, RN>(d, Ab, 1, ak, Bb, bk, bn, rs, true, K, Mt, Nt,
-                                                     m0, n0, g, t);
+                        if constexpr (std::is_same<E, BfPair>::value) {
+                                // k-paired operator copy, each block at twice its offset
+                                const E *op = ops + 2 * opoff[gg];
+                                const E *Ab = ax == 0 ? op : tin;
+                                const E *Bb = ax == 0 ? tin : op;
+                                // the operator is A' exactly when (ax == 0) != swap
+                                if (swap) {
+                                        if (ax == 0)
+                                                warp_tile_x3_pk<RM, RN, false, true>(d, Bb, bn, bk, Ab, ak, 1, rs,
+                                                                                     false, K, Mt, Nt, m0, n0, g, t);
+                                        else
+                                                warp_tile_x3_pk<RM, RN, true, false>(d, Bb, bn, bk, Ab, ak, 1, rs,
+                                                                                     false, K, Mt, Nt, m0, n0, g, t);
+                                } else {
+                                        if (ax == 0)
+                                                warp_tile_x3_pk<RM, RN, true, false>(d, Ab, 1, ak, Bb, bk, bn, rs,
+                                                                                     true, K, Mt, Nt, m0, n0, g, t);
+                                        else
+                                                warp_tile_x3_pk<RM, RN, false, true>(d, Ab, 1, ak, Bb, bk, bn, rs,
+                                                                                     true, K, Mt, Nt, m0, n0, g, t);
+                                }
+                        } else {
+                                const E *op = ops + opoff[gg];
+                                const E *Ab = ax == 0 ? op : tin;
+                                const E *Bb = ax == 0 ? tin : op;
+                                if (swap)
+                                        warp_tile_x3<RM, RN>(d, Bb, bn, bk, Ab, ak, 1, rs, false, K, Mt, Nt,
+                                                             m0, n0, g, t);
+                                else
+                                        warp_tile_x3<RM, RN>(d, Ab, 1, ak, Bb, bk, bn, rs, true, K, Mt, Nt,
+                                                             m0, n0, g, t);
+                        }
                 }
                 const float sc = (!ACC && scale) ? scale[g0] : 1.f;
                 OutT *Cb = out + (ACC ? 0 : g0 * out_gs);
@@ -1955,6 +2086,52 @@ __global__ void split_bf16_kernel(const double *__restrict__ a, BfPair *__restri
                         __double2bfloat16(v - (double) bf16_value(hi)));
                 b[i] = BfPair{hi | (lo << 16)};
         }
+}
+
+// The k-paired BF16 operator copy: job {src, -, rows, cols} (the plan's list
+// of referenced operator blocks) writes block (rows x cols, column-major at
+// src) at 2*src as (k/2)*2*rows + 2*r + (k%2), an odd cols padded with a
+// zero column (the block's doubled slot has room: cols+1 <= 2*cols).
+__global__ void pair_bf16_ops_kernel(const double *__restrict__ ops, BfPair *__restrict__ out,
+                                     const int64_t *__restrict__ jobs, int64_t njobs, int64_t n_ops,
+                                     int *err)
+{
+        for (int64_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+                const int64_t src = jobs[4 * j];
+                const int rows = (int) jobs[4 * j + 2], cols = (int) jobs[4 * j + 3];
+                const int kp = (cols + 1) & ~1;
+                if (rows < 0 || cols < 0 || src < 0 || src + (int64_t) rows * cols > n_ops) {
+                        if (threadIdx.x == 0) atomicExch(err, 6);
+                        continue;
+                }
+                const int n = rows * kp;
+                for (int p = threadIdx.x; p < n; p += blockDim.x) {
+                        const int pi = p / (2 * rows), rem = p - pi * 2 * rows;
+                        const int r = rem >> 1, k = 2 * pi + (rem & 1);
+                        const double v = k < cols ? ops[src + r + (int64_t) k * rows] : 0.0;
+                        const uint32_t hi = (uint32_t) __bfloat16_as_ushort(__double2bfloat16(v));
+                        const uint32_t lo = (uint32_t) __bfloat16_as_ushort(
+                                __double2bfloat16(v - (double) bf16_value(hi)));
+                        out[2 * src + p] = BfPair{hi | (lo << 16)};
+                }
+        }
+}
+
+int build_paired_bf16_ops(const HostPlan &hp, DevicePlan &dp, const int64_t *d_jobs, cudaStream_t s)
+{
+        const int64_t njobs = (int64_t) hp.tjobs.size() / 4;
+        if (njobs == 0) return T3NS_OK;
+        for (int64_t j = 0; j < njobs; ++j) {
+                const int64_t *jb = &hp.tjobs[4 * j];
+                if (jb[2] < 0 || jb[3] < 0 || jb[0] < 0 || jb[0] + jb[2] * jb[3] > hp.op_elems)
+                        return set_error(T3NS_E_ARG, "paired operators: job " + std::to_string(j) +
+                                                             " out of range");
+        }
+        const int grid = (int) std::min<int64_t>(njobs, 148 * 16);
+        pair_bf16_ops_kernel<<<grid, 256, 0, s>>>(dp.ops, reinterpret_cast<BfPair *>(dp.ops_bf16),
+                                                  d_jobs, njobs, hp.op_elems, dp.err);
+        T3NS_CUDA_TRY(cudaGetLastError());
+        return T3NS_OK;
 }
 
 int convert_to_bf16_pairs(const double *a, void *b, int64_t n, cudaStream_t s)

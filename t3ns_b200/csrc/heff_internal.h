@@ -130,7 +130,8 @@ struct DevicePlan {
         int64_t *toff = nullptr;                  // their offsets per task and axis
         float2 *ops_split = nullptr;              // {hi, lo} TF32 split of the operators
         float2 *x_split = nullptr;                // {hi, lo} split of the matvec input
-        uint32_t *ops_bf16 = nullptr;             // {hi, lo} BF16 pairs of the operators
+        uint32_t *ops_bf16 = nullptr;             // k-paired {hi, lo} BF16 copy of the operators
+                                                  // (2 * op_elems pairs, block at twice its offset)
         uint32_t *x_bf16 = nullptr;               // and of the matvec input
         int64_t *blk_off = nullptr;
         int4 *edims = nullptr;
@@ -162,6 +163,10 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
 int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s);
 // {hi, lo} BF16 pairs (hi in the low 16 bits) of n doubles.
 int convert_to_bf16_pairs(const double *a, void *b, int64_t n, cudaStream_t s);
+// Fills dp.ops_bf16 (2 * op_elems pairs) with the k-paired BF16 copy of every
+// referenced operator block (the plan's transposition job list).
+int build_paired_bf16_ops(const HostPlan &hp, DevicePlan &dp, const int64_t *d_jobs,
+                          cudaStream_t s);
 // {hi, lo} pairs of the transposed operators.
 int convert_to_pairs(const double *a, float2 *b, int64_t n, cudaStream_t s);
 // Fills dp.ops_t from dp.ops with the plan's transposition jobs.

@@ -86,12 +86,14 @@ def estimate_bytes(desc: StepDesc, precision: int, max_vecs: int = 30) -> int:
     return int(native.load().t3ns_server_estimate_bytes(C.byref(desc.desc), precision, max_vecs))
 
 
-def request_steps() -> list[str]:
-    """Captured steps that carry the reference's diagonal, Davidson guess and
-    Davidson energy (so every result is checked against the reference)."""
+def request_steps(patterns: list[str]) -> list[str]:
+    """Step files matching the glob `patterns` (the caller's request
+    sources) that carry a diagonal, a Davidson guess and a Davidson energy,
+    so every result can be checked against the energy recorded with it."""
     out = []
-    cands = sorted(glob.glob(os.path.join(ROOT, "oracle", "_ref", "captures", "*", "step_*.t3c")))
-    cands += sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.t3c")))
+    cands = []
+    for pat in patterns:
+        cands += sorted(glob.glob(pat))
     for p in cands:
         if os.path.getsize(p) < (256 << 20) and "eig.energy" in read_step(p):
             out.append(p)

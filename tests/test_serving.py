@@ -1,13 +1,17 @@
 """The engine's request loop (t3ns_server_*): admission against a device
 memory budget, concurrent solves, and the same result for a request alone
 and in a mix of concurrent requests."""
+import os
+
 import numpy as np
 import pytest
 
+from conftest import ROOT
 from t3ns_b200 import native
 from t3ns_b200.serving import Server, Workload, estimate_bytes, request_steps, run_stream
 
-STEPS = [p for p in request_steps() if "eig.energy" in Workload(p).step]
+STEPS = request_steps([os.path.join(ROOT, "oracle", "_ref", "captures", "*", "step_*.t3c"),
+                       os.path.join(ROOT, "tests", "golden", "*.t3c")])
 
 
 def test_estimate_covers_operators_and_basis():
