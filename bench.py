@@ -344,16 +344,21 @@ def sweep_comparison(timeout=900):
             r = subprocess.run([exe, *args, "--init", "c"], capture_output=True, text=True,
                                env=env, timeout=timeout)
             if r.returncode != 0:
-                return {"error": f"{name} {prec}: exit {r.returncode}"}
+                tail = (r.stdout + r.stderr).strip().splitlines()[-3:]
+                rec[prec] = {"error": f"exit {r.returncode}: " + " | ".join(tail)}
+                continue
             rec[prec] = parse_sweep_run(r.stdout)
-        f, m = rec["fp64"], rec["3xtf32"]
-        rec["speedup_mixed_vs_fp64"] = f["sweep_seconds"] / m["sweep_seconds"]
-        rec["matvec_bucket_speedup_mixed_vs_fp64"] = (
-            f["timers"].get("Heff T3NS: matvec", 0) + f["timers"].get("Heff DMRG: matvec", 0)) / max(
-            m["timers"].get("Heff T3NS: matvec", 0) + m["timers"].get("Heff DMRG: matvec", 0), 1e-12)
-        rec["abs_dE_mixed_vs_fp64"] = abs(m["energy"] - f["energy"])
-        rec["speedup_bf16x3_vs_fp64"] = f["sweep_seconds"] / rec["bf16x3"]["sweep_seconds"]
-        rec["abs_dE_bf16x3_vs_fp64"] = abs(rec["bf16x3"]["energy"] - f["energy"])
+        f = rec["fp64"]
+        if "error" not in f:
+            for prec, key in (("3xtf32", "mixed"), ("bf16x3", "bf16x3")):
+                m = rec[prec]
+                if "error" in m:
+                    continue
+                rec[f"speedup_{key}_vs_fp64"] = f["sweep_seconds"] / m["sweep_seconds"]
+                rec[f"matvec_bucket_speedup_{key}_vs_fp64"] = (
+                    f["timers"].get("Heff T3NS: matvec", 0) + f["timers"].get("Heff DMRG: matvec", 0)) / max(
+                    m["timers"].get("Heff T3NS: matvec", 0) + m["timers"].get("Heff DMRG: matvec", 0), 1e-12)
+                rec[f"abs_dE_{key}_vs_fp64"] = abs(m["energy"] - f["energy"])
         out[name] = rec
     out["note"] = ("timers are the reference's own buckets over the whole scheme "
                    "(src/optimize_network.c:43-95): 'Heff ...: matvec' is the Davidson solves, "

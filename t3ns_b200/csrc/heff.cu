@@ -1125,40 +1125,48 @@ heff_kernel(const T *__restrict__ x, double *__restrict__ y,
                                                 OPOFF[s * kGMax + tid] = tk.op_off[ax[s]] + row0[ax[s]];
                                         PREF[tid] = (Scale) tk.pref;
                                 }
+                                // Terms that apply the same first-stage operator share its
+                                // result (the host sorts a pair's terms so they sit next to
+                                // each other): while the first warps stage the group's
+                                // offsets, warp 2 reads the candidates' first-stage
+                                // operators itself, numbers their runs and takes the longest
+                                // prefix of the candidates whose n1 first-stage results and
+                                // g second-stage results fit the intermediate buffer, so one
+                                // barrier serves both.
+                                if (nst == 3 && (tid >> 5) == 2) {
+                                        const int lane = tid & 31;
+                                        int base = 0, gsel = 0, n1 = 0;
+                                        int64_t carry = -1;
+                                        for (int h = 0; h < kGMax / 32; ++h) {
+                                                const int t = lane + 32 * h;
+                                                const bool in = t < cand;
+                                                const int64_t cur =
+                                                        in ? tasks[pr.t0 + t0 + t].op_off[ax[0]] + row0[ax[0]] : -2;
+                                                int64_t prev = __shfl_up_sync(0xffffffffu, cur, 1);
+                                                if (lane == 0) prev = carry;
+                                                carry = __shfl_sync(0xffffffffu, cur, 31);
+                                                const bool first = in && (t == 0 || cur != prev);
+                                                const unsigned fb = __ballot_sync(0xffffffffu, first);
+                                                const int incl = base + __popc(fb & (0xffffffffu >> (31 - lane)));
+                                                const bool fits = in && (int64_t) incl * s1 +
+                                                                        (int64_t) (t + 1) * s2 <= C::kW;
+                                                const unsigned ok = __ballot_sync(0xffffffffu, fits);
+                                                if (in) AIDX[t] = incl - 1;
+                                                if (first) UOFF[incl - 1] = cur;
+                                                if (ok) {
+                                                        const int last = 31 - __clz(ok);
+                                                        gsel = 32 * h + last + 1;
+                                                        n1 = __shfl_sync(0xffffffffu, incl, last);
+                                                }
+                                                base += __popc(fb);
+                                        }
+                                        if (lane == 0) {
+                                                UNIT[1] = gsel;
+                                                UNIT[2] = n1;
+                                        }
+                                }
                                 __syncthreads();
                                 if (nst == 3) {
-                                        // Terms that apply the same first-stage operator share
-                                        // its result (the host sorts a pair's terms so they sit
-                                        // next to each other): warp 0 numbers the runs of equal
-                                        // first-stage operators and takes the longest prefix of
-                                        // the candidates whose n1 first-stage results and g
-                                        // second-stage results fit the intermediate buffer.
-                                        if (tid < 32) {
-                                                int base = 0, gsel = 0, n1 = 0;
-                                                for (int h = 0; h < kGMax / 32; ++h) {
-                                                        const int t = tid + 32 * h;
-                                                        const bool in = t < cand;
-                                                        const bool first = in && (t == 0 || OPOFF[t] != OPOFF[t - 1]);
-                                                        const unsigned fb = __ballot_sync(0xffffffffu, first);
-                                                        const int incl = base + __popc(fb & (0xffffffffu >> (31 - tid)));
-                                                        const bool fits = in && (int64_t) incl * s1 +
-                                                                                (int64_t) (t + 1) * s2 <= C::kW;
-                                                        const unsigned ok = __ballot_sync(0xffffffffu, fits);
-                                                        if (in) AIDX[t] = incl - 1;
-                                                        if (first) UOFF[incl - 1] = OPOFF[t];
-                                                        if (ok) {
-                                                                const int last = 31 - __clz(ok);
-                                                                gsel = 32 * h + last + 1;
-                                                                n1 = __shfl_sync(0xffffffffu, incl, last);
-                                                        }
-                                                        base += __popc(fb);
-                                                }
-                                                if (tid == 0) {
-                                                        UNIT[1] = gsel;
-                                                        UNIT[2] = n1;
-                                                }
-                                        }
-                                        __syncthreads();
                                         g = UNIT[1];
                                         const int n1 = UNIT[2];
                                         T *V2 = W + n1 * s1;
