@@ -663,7 +663,11 @@ int davidson_run(t3ns_heff *h, double *d_result, double *energy, int max_vecs,
         // (and 10) to the FP64 phase
         t3ns_davidson_info i1{}, i2{};
         const auto t0 = std::chrono::steady_clock::now();
-        const int split_its = std::max(1, max_its - std::max(10, max_its / 4));
+        int split_its = std::max(1, max_its - std::max(10, max_its / 4));
+        // a vector shorter than the basis: the split phase stops before its
+        // basis could span the whole space (the next correction would then
+        // vanish in the orthogonalisation), the FP64 phase finishes
+        if (h->hp.size <= max_vecs) split_its = (int) std::max<int64_t>(1, std::min<int64_t>(split_its, h->hp.size - 2));
         const double level = h->precision == T3NS_PREC_BF16X3 ? kStallLevelBf16 : kStallLevel;
         int rc = davidson_core(h->hp.size, matvec_in(h->precision), d_result, energy, max_vecs,
                                keep, tol, split_its, d_diag, &i1, s, /*stall=*/4, graphs, h->dp.err,
