@@ -225,6 +225,7 @@ static int create_impl(const t3ns_heff_desc *desc, int precision, t3ns_heff *h)
         T3NS_TRY(dev_alloc(h, &h->stage_y, (size_t) hp.size));
         T3NS_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         T3NS_TRY(upload_tiles(h, cfg));
+        if (kCfgs[cfg].bf16) T3NS_TRY(upload_tiles(h, cfg - kBfFirst));
         dp.active = cfg;
         return setup_precision(h, precision);
 }
@@ -336,6 +337,9 @@ int t3ns_heff_set_config(t3ns_heff *h, int config)
                                                      " does not run this precision "
                                                      "(3, 4: FP64 and 3xTF32; 5-7: BF16x3)");
         T3NS_TRY(upload_tiles(h, config));
+        // the other modes (FP64 defect correction) run a BF16x3-only
+        // configuration's launch shape in its FP64 twin
+        if (kCfgs[config].bf16) T3NS_TRY(upload_tiles(h, config - kBfFirst));
         h->dp.active = config;
         return T3NS_OK;
 }

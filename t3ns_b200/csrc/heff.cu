@@ -2163,23 +2163,30 @@ int convert_to_split(const double *a, float2 *b, int64_t n, cudaStream_t s)
 int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y, cudaStream_t s,
                 int *launches, bool per_block)
 {
+        // a BF16x3-only configuration (5-7) runs the other arithmetic modes in
+        // the configuration of the same launch shape (0-2), whose tiling the
+        // engine builds beside it (FP64 defect correction after BF16x3)
+        int act = dp.active;
+        if (act >= kBfFirst && !cfg_supports(act, precision) && dp.tiles[act - kBfFirst].built)
+                act -= kBfFirst;
         if (per_block) {
                 // the same kernel, one launch per output block (its own unit run)
-                const DeviceTiles &full = dp.tiles[dp.active];
+                const DeviceTiles &full = dp.tiles[act];
                 if (!full.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
-                if (precision != T3NS_PREC_FP64 || !cfg_supports(dp.active, precision))
+                if (precision != T3NS_PREC_FP64 || !cfg_supports(act, precision))
                         return set_error(T3NS_E_ARG, "matvec: per-block dispatch is FP64 only");
                 T3NS_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * dp.size, s));
                 DevicePlan one = dp;
+                one.active = act;
                 int n = 0;
                 for (size_t r = 0; r + 1 < full.block_runs.size(); r += 2) {
-                        DeviceTiles &dt = one.tiles[dp.active];
+                        DeviceTiles &dt = one.tiles[act];
                         dt.units = full.units + full.block_runs[r];
                         dt.n_units = full.block_runs[r + 1] - full.block_runs[r];
                         dt.grid = std::max(1, std::min(dt.n_units, full.grid));
                         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
                         int rc;
-                        switch (dp.active) {
+                        switch (act) {
                         case 0: rc = launch_cfg<CfgLarge, double>(one, dt, x, dp.ops, y, s); break;
                         case 1: rc = launch_cfg<CfgSmall, double>(one, dt, x, dp.ops, y, s); break;
                         case 2: rc = launch_cfg<CfgWide, double>(one, dt, x, dp.ops, y, s); break;
@@ -2192,14 +2199,14 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
                 if (launches) *launches = n;
                 return T3NS_OK;
         }
-        const DeviceTiles &dt = dp.tiles[dp.active];
+        const DeviceTiles &dt = dp.tiles[act];
         if (!dt.built) return set_error(T3NS_E_ARG, "matvec: the active configuration has no tiling");
         const bool split = precision == T3NS_PREC_3XTF32;
         const bool bf = precision == T3NS_PREC_BF16X3;
-        if (split && !kCfgs[dp.active].v2 && (!dp.ops_split || !dp.x_split))
+        if (split && !kCfgs[act].v2 && (!dp.ops_split || !dp.x_split))
                 return set_error(T3NS_E_ARG, "matvec: split precision is not set up on this plan");
-        if (!cfg_supports(dp.active, precision))
-                return set_error(T3NS_E_ARG, "matvec: configuration " + std::to_string(dp.active) +
+        if (!cfg_supports(act, precision))
+                return set_error(T3NS_E_ARG, "matvec: configuration " + std::to_string(act) +
                                                      " does not run this precision");
         if (bf && (!dp.ops_bf16 || !dp.x_bf16))
                 return set_error(T3NS_E_ARG, "matvec: BF16x3 is not set up on this plan");
@@ -2209,21 +2216,21 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
         if (launches) *launches = 0;
         if (dt.n_units == 0) return T3NS_OK;
         // the contraction-ordered kernel splits the staged blocks itself
-        if (split && !kCfgs[dp.active].v2) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
+        if (split && !kCfgs[act].v2) T3NS_TRY(convert_to_split(x, dp.x_split, dp.size, s));
         if (bf) T3NS_TRY(convert_to_bf16_pairs(x, dp.x_bf16, dp.size, s));
         T3NS_CUDA_TRY(cudaMemsetAsync(dp.counter, 0, sizeof(int), s));
         static_assert(kNumCfgs == 8, "one launch branch per configuration");
         int rc;
-        if (dp.active == 3) {
+        if (act == 3) {
                 rc = split ? launch_v2<CfgV2Wide, true>(dp, dt, x, y, s)
                            : launch_v2<CfgV2Wide, false>(dp, dt, x, y, s);
-        } else if (dp.active == 4) {
+        } else if (act == 4) {
                 rc = split ? launch_v2<CfgV2Large, true>(dp, dt, x, y, s)
                            : launch_v2<CfgV2Large, false>(dp, dt, x, y, s);
         } else if (bf) {
                 const BfPair *xs = reinterpret_cast<const BfPair *>(dp.x_bf16);
                 const BfPair *os = reinterpret_cast<const BfPair *>(dp.ops_bf16);
-                switch (dp.active) {
+                switch (act) {
                 case 0: rc = launch_cfg<CfgLarge, BfPair>(dp, dt, xs, os, y, s); break;
                 case 1: rc = launch_cfg<CfgSmall, BfPair>(dp, dt, xs, os, y, s); break;
                 case 2: rc = launch_cfg<CfgWide, BfPair>(dp, dt, xs, os, y, s); break;
@@ -2233,16 +2240,16 @@ int launch_heff(const DevicePlan &dp, int precision, const double *x, double *y,
                 }
         } else if (split) {
                 const float2 *xs = dp.x_split, *os = dp.ops_split;
-                rc = dp.active == 0   ? launch_cfg<CfgLarge, float2>(dp, dt, xs, os, y, s)
-                     : dp.active == 1 ? launch_cfg<CfgSmall, float2>(dp, dt, xs, os, y, s)
+                rc = act == 0   ? launch_cfg<CfgLarge, float2>(dp, dt, xs, os, y, s)
+                     : act == 1 ? launch_cfg<CfgSmall, float2>(dp, dt, xs, os, y, s)
                                       : launch_cfg<CfgWide, float2>(dp, dt, xs, os, y, s);
         } else {
-                rc = dp.active == 0   ? launch_cfg<CfgLarge, double>(dp, dt, x, dp.ops, y, s)
-                     : dp.active == 1 ? launch_cfg<CfgSmall, double>(dp, dt, x, dp.ops, y, s)
+                rc = act == 0   ? launch_cfg<CfgLarge, double>(dp, dt, x, dp.ops, y, s)
+                     : act == 1 ? launch_cfg<CfgSmall, double>(dp, dt, x, dp.ops, y, s)
                                       : launch_cfg<CfgWide, double>(dp, dt, x, dp.ops, y, s);
         }
         T3NS_TRY(rc);
-        if (launches) *launches = ((split && !kCfgs[dp.active].v2) || bf) ? 2 : 1;
+        if (launches) *launches = ((split && !kCfgs[act].v2) || bf) ? 2 : 1;
         return T3NS_OK;
 }
 

@@ -92,3 +92,23 @@ def test_bf16x3_davidson_defect_corrected(path, torch_cuda):
     r = fp64.matvec_host(res) - e * res
     assert np.linalg.norm(r) <= tol * 1.01
     fp64.close()
+
+
+@pytest.mark.parametrize("config", [5, 6, 7])
+def test_bf16x3_only_config_runs_fp64_defect_correction(config, torch_cuda):
+    """With a BF16x3-only configuration active, the FP64 iterations of the
+    defect correction (and FP64 matvecs after switching back) run in the
+    configuration of the same launch shape."""
+    cands = [p for p in STEPS if "eig.energy" in read_step(p)]
+    s = read_step(cands[len(cands) // 2])
+    plan = HeffPlan(StepDesc(s), T3NS_PREC_BF16X3)
+    plan.set_config(config)
+    res = s["eig.guess"].copy()
+    tol = float(s["eig.tol"][0])
+    e, ret, info = plan.davidson_host(res, s["diag"], tol=tol, max_its=int(s["eig.max_its"][0]),
+                                      max_vecs=int(s["eig.max_vecs"][0]),
+                                      keep=int(s["eig.keep"][0]))
+    assert info["fp64_iterations"] >= 1
+    assert abs(e - float(s["eig.energy"][0])) <= ENERGY_TOL
+    assert plan.config() == config
+    plan.close()
